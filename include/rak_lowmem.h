@@ -1,0 +1,203 @@
+/*
+ * rak_lowmem.h -- C ABI of the B200-native memory-efficient label propagation library
+ * (librak_lowmem.so): νMG-LPA (weighted Misra-Gries sketch, 2..16 slots; νMG8 = 8 slots) and
+ * νBM-LPA (weighted Boyer-Moore vote) community detection on one GPU.
+ *
+ * The reference exposes its path as C++ templates; each entry point below names the reference
+ * interface it replaces (paths relative to the reference repository):
+ *   rak_lowmem_cuda        <- rakLowmemStaticCuda<SLOTS>(x, o)        inc/rakLowmemCuda.hxx:624-632
+ *                             rakLowmemInvokeCuda(x, o, fi, fm)       inc/rakLowmemCuda.hxx:538-607
+ *   rak_graph_create/run   <- the setup half (partition + CSR upload, :562-583) and the timed
+ *                             loop half (:586-595) of rakLowmemInvokeCuda, split so a graph can
+ *                             stay resident on the device across calls
+ *   rak_graph_step         <- one move iteration, rakLowmemLoopCuU body  inc/rakLowmemCuda.hxx:476-487
+ *   rak_modularity_f64     <- modularityBy(x, fc, M, R=1)            inc/properties.hxx:177-192
+ *   rak_options            <- RakOptions{repeat,tolerance,maxIterations} inc/rak.hxx:19-40
+ *   rak_result             <- RakResult<K>{membership,iterations,time,markingTime,
+ *                             initializationTime,memory}             inc/rak.hxx:53-97
+ *
+ * Conventions. Every call returns a rak_status and never exits the process (the reference
+ * prints and calls exit(), inc/_cuda.hxx:221-235). Vertex ids and labels are 0-based uint32.
+ * Membership labels are vertex ids of the original graph (the reference returns indices into its
+ * degree-partitioned order, inc/rakLowmemCuda.hxx:597-598; both are arbitrary community names).
+ * A context is bound to one device and one stream and is not thread-safe; use one per thread.
+ */
+#ifndef RAK_LOWMEM_H
+#define RAK_LOWMEM_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RAK_ABI_VERSION 1
+
+typedef enum rak_status {
+  RAK_OK = 0,
+  RAK_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad option value, size out of range */
+  RAK_ERR_INVALID_CSR = 2,      /* offsets not monotone / not ending at m, target id >= n */
+  RAK_ERR_OUT_OF_MEMORY = 3,    /* device or host allocation failed, or admission budget exceeded */
+  RAK_ERR_CUDA = 4,             /* a CUDA runtime call failed; see rak_ctx_last_error */
+  RAK_ERR_TIMEOUT = 5,          /* a bounded device-side wait gave up */
+  RAK_ERR_NO_DEVICE = 6,        /* no CUDA device, or the device is not sm_100 */
+  RAK_ERR_UNSUPPORTED = 7,      /* option combination not implemented */
+  RAK_ERR_BUSY = 8              /* serving: request queue full */
+} rak_status;
+
+typedef enum rak_location { RAK_HOST = 0, RAK_DEVICE = 1 } rak_location;
+
+typedef enum rak_mode {
+  /* In-place (Gauss-Seidel) label and flag updates, as the reference GPU path does
+   * (inc/rakLowmemCuda.hxx:153,311,413). Split per-vertex sketches for high-degree vertices.
+   * Defaults follow the reference GPU loop: pickless every 8th iteration, tolerance test
+   * skipped on pickless iterations, no rescan. Nondeterministic, like the reference. */
+  RAK_MODE_ASYNC = 0,
+  /* Synchronous (Jacobi) iterations from a label snapshot, with every vertex scanned exactly in
+   * edge order: bit-identical, iteration by iteration, to the reference's CPU per-vertex
+   * functions (inc/rakLowmem.hxx:63-172) run on the same snapshot. Defaults follow the reference
+   * CPU loop: rescan on, no pickless, tolerance tested every iteration. */
+  RAK_MODE_SYNC = 1,
+  /* Synchronous iterations with the split per-vertex sketches of RAK_MODE_ASYNC: deterministic,
+   * and bit-identical to the documented split layout (rak_options.lane_max/hub_min/hub_chunk). */
+  RAK_MODE_SYNC_SPLIT = 2
+} rak_mode;
+
+/* A graph in CSR form. All three arrays live in `location`. The graph should be symmetric
+ * (undirected, both directions stored) as the reference's driver makes it (main.cxx:119). */
+typedef struct rak_csr {
+  int64_t n;              /* vertices, < 2^31 */
+  int64_t m;              /* directed edges, == offsets[n] */
+  int32_t offset_bits;    /* 32 or 64: element type of offsets */
+  int32_t location;       /* rak_location */
+  const void *offsets;    /* n+1 entries, offsets[0] == 0 */
+  const uint32_t *targets;/* m entries, each < n */
+  const float *weights;   /* m entries, or NULL for unit weights */
+} rak_csr;
+
+typedef struct rak_options {
+  int32_t repeat;             /* RakOptions::repeat: runs averaged into time_ms [1] */
+  double tolerance;           /* RakOptions::tolerance: stop when changed/n <= tolerance [0.05] */
+  int32_t max_iterations;     /* RakOptions::maxIterations [20], <= 1024 */
+  int32_t slots;              /* 1: νBM-LPA; 2, 4, 8, 16: νMG-LPA with that many slots [8] */
+  int32_t mode;               /* rak_mode [RAK_MODE_ASYNC] */
+  int32_t rescan;             /* -1: mode default; 1: exact weights of sketch keys (SYNC only) */
+  int32_t pickless_step;      /* -1: mode default; 0: never; k: iterations l%k==0 only move to
+                                 smaller labels (inc/rakLowmemCuda.hxx:473-476) */
+  int32_t check_on_pickless;  /* -1: mode default; 1: tolerance tested on pickless iterations */
+  int32_t lane_max;           /* 0: default; split layout, one lane per vertex up to this degree */
+  int32_t hub_min;            /* 0: default; vertices above this degree are split into chunks */
+  int32_t hub_chunk;          /* 0: default; edges per chunk of a split vertex */
+  int32_t validate;           /* 1: check the CSR on the device first [1] */
+  int32_t compute_modularity; /* 1: fill rak_result.modularity (FP64 kernel) [0] */
+  int32_t start_iteration;    /* iteration index of the first step (pickless schedule) [0] */
+  const uint8_t *initial_flags; /* NULL: every vertex affected; else n flags in the csr's location */
+  int64_t reserved[8];
+} rak_options;
+
+typedef struct rak_result {
+  int32_t iterations;          /* RakResult::iterations */
+  float time_ms;               /* RakResult::time: init + mark + iterations, device time, averaged */
+  float marking_time_ms;       /* RakResult::markingTime */
+  float initialization_time_ms;/* RakResult::initializationTime */
+  float memory_gb;             /* RakResult::memory: working buffers beyond the graph, in GB */
+  float plan_ms;               /* degree bucketing of the graph on the device (once per graph) */
+  float h2d_ms;                /* host->device copies inside this call (host-located csr) */
+  float d2h_ms;                /* device->host copy of the membership (host-located csr) */
+  uint64_t peak_device_bytes;  /* all device memory this call held at once, graph included */
+  uint64_t traversed_edges;    /* sum over iterations of the degrees of the vertices processed */
+  uint64_t processed_vertices; /* sum over iterations of the vertices processed */
+  uint64_t changed_last;       /* vertices that changed label in the last iteration */
+  double modularity;           /* when requested, else NaN */
+} rak_result;
+
+typedef struct rak_ctx rak_ctx;
+typedef struct rak_graph rak_graph;
+
+/* ---- library ---------------------------------------------------------------------------- */
+int rak_abi_version(void);
+const char *rak_status_string(rak_status s);
+/* Fills the defaults documented above. */
+void rak_options_default(rak_options *o);
+
+/* ---- context ---------------------------------------------------------------------------- */
+/* Binds to `device` (must be sm_100). No reference counterpart: the reference uses the default
+ * device and stream (inc/rakLowmemCuda.hxx:570). */
+rak_status rak_ctx_create(int device, rak_ctx **out);
+rak_status rak_ctx_destroy(rak_ctx *ctx);
+/* Work is issued on `stream` (a cudaStream_t; NULL = the context's own stream). */
+rak_status rak_ctx_set_stream(rak_ctx *ctx, void *stream);
+/* Text of the last error on this context (empty if none). */
+const char *rak_ctx_last_error(const rak_ctx *ctx);
+
+/* ---- single graph ----------------------------------------------------------------------- */
+/* rakLowmemStaticCuda<SLOTS>(x, o) / rakLowmemInvokeCuda(x, o, fi, fm): one complete run.
+ * q: initial labels (NULL: identity, as rakInitializeCuW does, inc/rakCuda.hxx:25-44), n entries.
+ * membership: n entries, written. q and membership are in g->location. Host graphs are copied
+ * to the device inside the call (h2d_ms) and freed before returning, as the reference does. */
+rak_status rak_lowmem_cuda(rak_ctx *ctx, const rak_csr *g, const uint32_t *q,
+                           const rak_options *o, uint32_t *membership, rak_result *res);
+
+/* Makes a device-resident copy of g (or binds a device-located g without copying) and builds
+ * its degree-bucket plan for the layout in o (NULL: defaults). */
+rak_status rak_graph_create(rak_ctx *ctx, const rak_csr *g, const rak_options *o, rak_graph **out);
+rak_status rak_graph_destroy(rak_graph *gr);
+/* Device bytes held by the resident graph (copy + plan). */
+uint64_t rak_graph_device_bytes(const rak_graph *gr);
+
+/* A complete run on a resident graph. q (may be NULL) and membership are device pointers. */
+rak_status rak_graph_run(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const rak_options *o,
+                         uint32_t *membership, rak_result *res);
+
+/* One move iteration with index `iteration` (pickless schedule) from the snapshot
+ * (vcom_prev, aff_prev) into (vcom_next, aff_next); all device pointers, n entries each.
+ * In RAK_MODE_ASYNC the update is in place on vcom_next/aff_next after copying prev into them.
+ * *changed receives the number of vertices that changed label. */
+rak_status rak_graph_step(rak_ctx *ctx, rak_graph *gr, const rak_options *o, int iteration,
+                          const uint32_t *vcom_prev, const uint8_t *aff_prev,
+                          uint32_t *vcom_next, uint8_t *aff_next, uint64_t *changed);
+
+/* modularityBy(x, membership, M=w(x)/2, R=1) accumulated in FP64 on the device.
+ * membership is in g->location. */
+rak_status rak_modularity_f64(rak_ctx *ctx, const rak_csr *g, const uint32_t *membership,
+                              double *q);
+
+/* ---- synthetic graphs (host, deterministic; for tests and benchmarks) -------------------- */
+/* A host CSR allocated by the library; free with rak_host_csr_free. */
+typedef struct rak_host_csr {
+  int64_t n, m;
+  int64_t *offsets;   /* n+1 */
+  uint32_t *targets;  /* m */
+  float *weights;     /* m, or NULL when unit weights were requested */
+  uint32_t *truth;    /* planted labels (SBM), or NULL */
+} rak_host_csr;
+
+/* Symmetric R-MAT: n*edge_factor samples, each quadrant step chosen with probabilities
+ * (a, b, c, 1-a-b-c); self-loops and duplicates removed, both directions stored. Weights are
+ * uniform in [w_lo, w_hi) per undirected pair (same value both ways); w_lo == w_hi == 1 gives
+ * NULL weights. threads <= 0: all cores. */
+rak_status rak_gen_rmat(int scale, double edge_factor, double a, double b, double c, uint64_t seed,
+                        float w_lo, float w_hi, int threads, rak_host_csr *out);
+/* Planted-partition SBM: n vertices in k equal blocks, expected degree avg_degree, ratio
+ * p_in/p_out; unit weights; truth[] holds the planted block of each vertex. */
+rak_status rak_gen_sbm(int64_t n, int64_t k, double avg_degree, double in_out_ratio, uint64_t seed,
+                       int threads, rak_host_csr *out);
+/* 2D 4-neighbour lattice of width x height, each undirected edge deleted with probability
+ * p_delete, plus shortcut_frac * (edges) random undirected shortcuts; unit weights. */
+rak_status rak_gen_lattice(int64_t width, int64_t height, double p_delete, double shortcut_frac,
+                           uint64_t seed, int threads, rak_host_csr *out);
+void rak_host_csr_free(rak_host_csr *g);
+
+/* Host-side CSR check (same rules as the device check): RAK_OK or RAK_ERR_INVALID_CSR. */
+rak_status rak_csr_validate_host(const rak_csr *g);
+
+/* Degree-bucket plan summary computed on the host from degrees (for tests and tooling):
+ * fills counts[0..7] = vertices per lane group size 1,2,4,8,16,32, hubs, isolated, and returns
+ * the number of hub chunks through *hub_chunks. */
+rak_status rak_plan_summary_host(const rak_csr *g, const rak_options *o, int64_t counts[8],
+                                 int64_t *hub_chunks);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

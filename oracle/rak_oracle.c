@@ -1,0 +1,276 @@
+/*
+ * rak_oracle.c -- TEST INFRASTRUCTURE ONLY (see rak_oracle.h).
+ *
+ * CPU restatement of the reference's memory-efficient label propagation:
+ *   - Misra-Gries accumulate          : inc/rakLowmem.hxx:63-89   (rakLowmemScanCommunityU)
+ *   - exact rescan and argmax          : inc/rakLowmem.hxx:151-172 (rakLowmemChooseCommunityW)
+ *   - weighted Boyer-Moore             : inc/rakLowmem.hxx:115-128 (rakLowmemScanCommunitiesMajority)
+ *   - move rule, marking, loop         : inc/rakLowmem.hxx:189-212, 257-260
+ *   - sketch merge by re-accumulation  : inc/sketchCuda.hxx:150-158 (sketchMergeWarpCudU)
+ *   - pickless rule                    : inc/rakLowmemCuda.hxx:473-487
+ *   - modularity                       : inc/properties.hxx:123-126, 177-192
+ * Floating point follows the reference exactly: float sketch weights, adds and subtracts only
+ * (no multiply, so no contraction), double modularity.
+ */
+#include "rak_oracle.h"
+#include <stdlib.h>
+#include <string.h>
+
+static float edge_w(const orc_csr *g, int64_t e) { return g->wt ? g->wt[e] : 1.0f; }
+
+void orc_sketch_clear(orc_sketch *s, int slots) {
+  for (int i = 0; i < slots; ++i) { s->k[i] = ORC_NONE; s->w[i] = 0.0f; }
+}
+
+/* inc/rakLowmem.hxx:63-89: add w to every slot holding c; if none held it, the LAST slot whose
+ * weight is zero takes (c, w); if no slot is free, every weight drops by w, clamped at zero. */
+void orc_mg_accumulate(orc_sketch *s, int slots, uint32_t c, float w) {
+  int has = 0;
+  for (int i = 0; i < slots; ++i)
+    if (s->k[i] == c) { s->w[i] += w; has = 1; }
+  if (has) return;
+  int f = -1;
+  for (int i = 0; i < slots; ++i)
+    if (s->w[i] == 0.0f) f = i;
+  if (f >= 0) { s->k[f] = c; s->w[f] = w; return; }
+  for (int i = 0; i < slots; ++i) {
+    float t = s->w[i] - w;
+    s->w[i] = t < 0.0f ? 0.0f : t;
+  }
+}
+
+/* inc/rakLowmem.hxx:120-126: weighted Boyer-Moore vote held in slot 0. */
+void orc_bm_accumulate(orc_sketch *s, uint32_t c, float w) {
+  if (c == s->k[0]) s->w[0] += w;
+  else if (s->w[0] > w) s->w[0] -= w;
+  else { s->k[0] = c; s->w[0] = w; }
+}
+
+/* inc/sketchCuda.hxx:150-158: merge b into a by re-accumulating b's non-zero slots in order. */
+void orc_sketch_merge(orc_sketch *a, const orc_sketch *b, int slots) {
+  if (slots == 1) {
+    if (b->w[0] != 0.0f) orc_bm_accumulate(a, b->k[0], b->w[0]);
+    return;
+  }
+  for (int j = 0; j < slots; ++j)
+    if (b->w[j] != 0.0f) orc_mg_accumulate(a, slots, b->k[j], b->w[j]);
+}
+
+/* inc/rakLowmem.hxx:164-171: linear argmax, strict '>', starting from weight 0. */
+void orc_sketch_choose(const orc_sketch *s, int slots, uint32_t *c, float *w) {
+  uint32_t cm = ORC_NONE;
+  float wm = 0.0f;
+  for (int i = 0; i < slots; ++i)
+    if (s->w[i] > wm) { wm = s->w[i]; cm = s->k[i]; }
+  *c = cm; *w = wm;
+}
+
+static void acc(orc_sketch *s, int slots, uint32_t c, float w) {
+  if (slots == 1) orc_bm_accumulate(s, c, w);
+  else orc_mg_accumulate(s, slots, c, w);
+}
+
+/* Sequential scan of edges [b, e) of u with stride st (self-loops skipped, rakLowmem.hxx:65). */
+static void scan_range(const orc_csr *g, uint32_t u, const uint32_t *vcom, int slots,
+                       int64_t b, int64_t e, int64_t st, orc_sketch *s) {
+  for (int64_t i = b; i < e; i += st) {
+    uint32_t v = g->tgt[i];
+    if (v == u) continue;
+    acc(s, slots, vcom[v], edge_w(g, i));
+  }
+}
+
+/* Fixed binary tree over lanes L[0..n): at each level lane s (< off) merges lane s+off. */
+static void tree_merge(orc_sketch *L, int n, int slots) {
+  for (int off = n / 2; off >= 1; off /= 2)
+    for (int s = 0; s < off; ++s) orc_sketch_merge(&L[s], &L[s + off], slots);
+}
+
+static int group_size(const orc_layout *ly, int64_t deg) {
+  int G = 2;
+  while (G < 32 && (int64_t)G * ly->lane_max < deg) G *= 2;
+  return G;
+}
+
+/* The split per-vertex sketch (documented in rak_oracle.h, orc_layout). */
+static void split_sketch(const orc_csr *g, const orc_opts *o, uint32_t u, const uint32_t *vcom,
+                         orc_sketch *out) {
+  const int S = o->slots;
+  const int64_t b = g->off[u], deg = g->off[u + 1] - g->off[u];
+  const orc_layout *ly = &o->layout;
+  orc_sketch L[32];
+  if (deg <= ly->lane_max) {
+    orc_sketch_clear(out, S);
+    scan_range(g, u, vcom, S, b, b + deg, 1, out);
+    return;
+  }
+  if (deg <= ly->hub_min) {
+    int G = group_size(ly, deg);
+    for (int s = 0; s < G; ++s) {
+      orc_sketch_clear(&L[s], S);
+      scan_range(g, u, vcom, S, b + s, b + deg, G, &L[s]);
+    }
+    tree_merge(L, G, S);
+    *out = L[0];
+    return;
+  }
+  const int64_t CH = ly->hub_chunk, nch = (deg + CH - 1) / CH;
+  orc_sketch *C = (orc_sketch *)malloc(sizeof(orc_sketch) * (size_t)nch);
+  for (int64_t j = 0; j < nch; ++j) {
+    int64_t cb = b + j * CH, ce = cb + CH < b + deg ? cb + CH : b + deg;
+    for (int s = 0; s < 32; ++s) {
+      orc_sketch_clear(&L[s], S);
+      scan_range(g, u, vcom, S, cb + s, ce, 32, &L[s]);
+    }
+    tree_merge(L, 32, S);
+    C[j] = L[0];
+  }
+  for (int l = 0; l < 32; ++l) {
+    orc_sketch_clear(&L[l], S);
+    for (int64_t j = l; j < nch; j += 32) orc_sketch_merge(&L[l], &C[j], S);
+  }
+  tree_merge(L, 32, S);
+  *out = L[0];
+  free(C);
+}
+
+/* inc/rakLowmem.hxx:154-162: exact weights of the sketch keys, summed in edge order. */
+static void rescan(const orc_csr *g, uint32_t u, const uint32_t *vcom, int slots, orc_sketch *s) {
+  for (int i = 0; i < slots; ++i) s->w[i] = 0.0f;
+  for (int64_t e = g->off[u]; e < g->off[u + 1]; ++e) {
+    uint32_t v = g->tgt[e];
+    if (v == u) continue;
+    uint32_t c = vcom[v];
+    float w = edge_w(g, e);
+    for (int i = 0; i < slots; ++i)
+      if (s->k[i] == c) s->w[i] += w;
+  }
+}
+
+void orc_choose(const orc_csr *g, const orc_opts *o, uint32_t u, const uint32_t *vcom,
+                uint32_t *c, float *w) {
+  orc_sketch s;
+  if (o->split) {
+    split_sketch(g, o, u, vcom, &s);
+  } else {
+    orc_sketch_clear(&s, o->slots);
+    scan_range(g, u, vcom, o->slots, g->off[u], g->off[u + 1], 1, &s);
+    if (o->rescan && o->slots > 1) rescan(g, u, vcom, o->slots, &s);
+  }
+  orc_sketch_choose(&s, o->slots, c, w);
+}
+
+static int is_pickless(const orc_opts *o, int l) { return o->pickless_step > 0 && l % o->pickless_step == 0; }
+
+/* Synchronous form of inc/rakLowmem.hxx:189-212: every decision reads the snapshot; a moved
+ * vertex marks its neighbours other than itself (the reference marks, then clears u). */
+uint64_t orc_sync_step(const orc_csr *g, const orc_opts *o, int iteration,
+                       const uint32_t *vcom_prev, const uint8_t *aff_prev,
+                       uint32_t *vcom_next, uint8_t *aff_next,
+                       uint64_t *edges_out, uint64_t *processed_out) {
+  const int pl = is_pickless(o, iteration);
+  uint64_t changed = 0, edges = 0, processed = 0;
+  memset(aff_next, 0, (size_t)g->n);
+  for (int64_t u = 0; u < g->n; ++u) vcom_next[u] = vcom_prev[u];
+  for (int64_t u = 0; u < g->n; ++u) {
+    if (!aff_prev[u]) continue;
+    int64_t deg = g->off[u + 1] - g->off[u];
+    if (deg == 0) continue;
+    ++processed; edges += (uint64_t)deg;
+    uint32_t d = vcom_prev[u], c; float w;
+    orc_choose(g, o, (uint32_t)u, vcom_prev, &c, &w);
+    if (!(w > 0.0f) || c == d) continue;
+    if (pl && c > d) continue;
+    vcom_next[u] = c; ++changed;
+    for (int64_t e = g->off[u]; e < g->off[u + 1]; ++e)
+      if (g->tgt[e] != (uint32_t)u) aff_next[g->tgt[e]] = 1;
+  }
+  if (edges_out) *edges_out += edges;
+  if (processed_out) *processed_out += processed;
+  return changed;
+}
+
+/* Loop of inc/rakLowmem.hxx:257-260 (tolerance test every iteration) with the optional
+ * pickless schedule of inc/rakLowmemCuda.hxx:473-487. */
+int orc_sync_run(const orc_csr *g, const orc_opts *o, const uint32_t *q, uint32_t *labels,
+                 uint64_t *edges_out) {
+  size_t n = (size_t)g->n;
+  uint32_t *a = (uint32_t *)malloc(n * 4 + 4), *b = (uint32_t *)malloc(n * 4 + 4);
+  uint8_t *fa = (uint8_t *)malloc(n + 1), *fb = (uint8_t *)malloc(n + 1);
+  for (size_t u = 0; u < n; ++u) { a[u] = q ? q[u] : (uint32_t)u; fa[u] = 1; }
+  int l = 0;
+  while (l < o->max_iterations) {
+    uint64_t ch = orc_sync_step(g, o, l, a, fa, b, fb, edges_out, NULL);
+    uint32_t *t = a; a = b; b = t;
+    uint8_t *tf = fa; fa = fb; fb = tf;
+    int pl = is_pickless(o, l);
+    ++l;
+    if ((!pl || o->check_on_pickless) && (double)ch / (double)g->n <= o->tolerance) break;
+  }
+  memcpy(labels, a, n * 4);
+  free(a); free(b); free(fa); free(fb);
+  return l;
+}
+
+/* inc/rakLowmem.hxx:189-212 and 228-264 with one thread: in-place updates in vertex order.
+ * Keys persist across vertices (the reference reuses one key array per thread and clears only
+ * the weights, rakLowmem.hxx:200); the first vertex starts from keys that match nothing. */
+int orc_serial_run(const orc_csr *g, int slots, int rescan_on, double tolerance, int max_iterations,
+                   uint32_t *labels) {
+  size_t n = (size_t)g->n;
+  uint8_t *aff = (uint8_t *)malloc(n + 1);
+  for (size_t u = 0; u < n; ++u) { labels[u] = (uint32_t)u; aff[u] = 1; }
+  orc_sketch s;
+  orc_sketch_clear(&s, ORC_MAX_SLOTS);
+  int l = 0;
+  for (l = 0; l < max_iterations;) {
+    uint64_t a = 0;
+    for (int64_t u = 0; u < g->n; ++u) {
+      if (!aff[u]) continue;
+      uint32_t d = labels[u], c; float w;
+      if (slots > 1) {
+        for (int i = 0; i < slots; ++i) s.w[i] = 0.0f;
+        scan_range(g, (uint32_t)u, labels, slots, g->off[u], g->off[u + 1], 1, &s);
+        if (rescan_on) rescan(g, (uint32_t)u, labels, slots, &s);
+        orc_sketch_choose(&s, slots, &c, &w);
+      } else {
+        orc_sketch bm; orc_sketch_clear(&bm, 1);
+        scan_range(g, (uint32_t)u, labels, 1, g->off[u], g->off[u + 1], 1, &bm);
+        c = bm.k[0]; w = bm.w[0];
+      }
+      if (w > 0.0f && c != d) {
+        labels[u] = c; ++a;
+        for (int64_t e = g->off[u]; e < g->off[u + 1]; ++e) aff[g->tgt[e]] = 1;
+      }
+      aff[u] = 0;
+    }
+    ++l;
+    if ((double)a / (double)g->n <= tolerance) break;
+  }
+  free(aff);
+  return l;
+}
+
+/* inc/properties.hxx:177-192 (per-edge cin/ctot in vertex then edge order) and :123-126. */
+double orc_modularity(const orc_csr *g, const uint32_t *labels) {
+  size_t n = (size_t)g->n;
+  double *cin = (double *)calloc(n + 1, sizeof(double)), *ctot = (double *)calloc(n + 1, sizeof(double));
+  double m2 = 0.0;
+  for (int64_t u = 0; u < g->n; ++u) {
+    uint32_t c = labels[u];
+    for (int64_t e = g->off[u]; e < g->off[u + 1]; ++e) {
+      double w = (double)edge_w(g, e);
+      if (labels[g->tgt[e]] == c) cin[c] += w;
+      ctot[c] += w;
+      m2 += w;
+    }
+  }
+  double q = 0.0;
+  if (m2 > 0.0)
+    for (size_t c = 0; c < n; ++c) {
+      double t = ctot[c] / m2;
+      q += cin[c] / m2 - t * t;
+    }
+  free(cin); free(ctot);
+  return q;
+}

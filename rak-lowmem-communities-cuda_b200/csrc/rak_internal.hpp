@@ -1,0 +1,111 @@
+// rak_internal.hpp -- declarations shared by the host orchestration (rak_host.cpp) and the CUDA
+// translation units. No CUDA device code here; plain structs passed to kernels by value.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace rak {
+
+// Work regions of the degree-bucket plan, in processing order. The plan's vertex list `order`
+// holds region 0's vertices first, then region 1's, and so on.
+//   region 0      : split vertices (degree > hub_min), one item per chunk of hub_chunk edges,
+//                   32 lanes per chunk
+//   regions 1..5  : lane groups of G = 32, 16, 8, 4, 2 lanes per vertex
+//   region 6      : one lane per vertex (1 <= degree <= lane_max), degree descending
+// Isolated vertices (degree 0) are in no region: they can never move.
+constexpr int NREG = 7;
+constexpr int REG_HUB = 0;
+constexpr int REG_LANE = 6;
+__host__ __device__ constexpr int region_group(int r) { return r == REG_LANE ? 1 : (r == REG_HUB ? 32 : (64 >> r)); }
+
+struct Regions {
+  int64_t vbegin[NREG];
+  int64_t vcount[NREG];
+  int64_t ibegin[NREG + 1];  // item prefix; ibegin[NREG] = total items
+};
+
+// Layout parameters (rak_options lane_max / hub_min / hub_chunk after defaults).
+struct Layout {
+  int64_t lane_max;
+  int64_t hub_min;
+  int64_t hub_chunk;
+};
+constexpr int64_t DEFAULT_LANE_MAX = 128;
+constexpr int64_t DEFAULT_HUB_MIN = 8192;
+constexpr int64_t DEFAULT_HUB_CHUNK = 4096;
+constexpr int64_t MAX_LANE_MAX = 1024;
+
+// Sort key of a vertex in the plan (regions in order, region 6 by degree descending);
+// key_isolated for degree 0. Shared by the device plan kernel and the host summary.
+__host__ __device__ inline uint32_t plan_key(int64_t deg, const Layout &ly) {
+  if (deg <= 0) return uint32_t(6 + ly.lane_max);
+  if (deg <= ly.lane_max) return uint32_t(6 + (ly.lane_max - deg));
+  if (deg > ly.hub_min) return 0u;
+  int G = 2;
+  while (G < 32 && int64_t(G) * ly.lane_max < deg) G *= 2;
+  // G = 32 -> region 1, 16 -> 2, 8 -> 3, 4 -> 4, 2 -> 5
+  int r = 1;
+  for (int g = 32; g > G; g >>= 1) ++r;
+  return uint32_t(r);
+}
+__host__ __device__ inline int key_region(uint32_t key) { return key < 6 ? int(key) : REG_LANE; }
+
+struct RunStateHost {
+  unsigned int bar, abort, error, iterations;
+};
+
+// Everything the persistent LPA kernel needs.
+struct LpaArgs {
+  const void *off;          // int32 or int64 offsets (template parameter of the kernel)
+  const uint32_t *tgt;
+  const float *wt;          // nullptr: unit weights
+  int64_t n;
+  const uint32_t *order;
+  Regions rg;
+  const uint32_t *chunk_hub;   // per chunk: index of its split vertex within region 0
+  const int64_t *hub_first;    // per split vertex: first chunk (nhub+1 entries)
+  int64_t hub_chunk;
+  int64_t nchunks;
+  uint32_t *vcom0, *vcom1;     // labels; vcom1 used by the synchronous modes
+  uint8_t *aff0, *aff1;        // affected flags; aff1 used by the synchronous modes
+  uint32_t *hub_arrive;        // per split vertex: chunks finished this iteration
+  uint32_t *hub_claim;         // per split vertex: (iteration+1)<<1 | active, asynchronous mode
+  int32_t *hub_moved;          // per split vertex: last iteration it moved in (-1: never)
+  uint32_t *sk_keys;           // per chunk: slots keys of its partial sketch
+  float *sk_wts;               // per chunk: slots weights
+  unsigned long long *stats;   // per iteration: changed, edges, processed, split vertices moved
+  void *rs;                    // RunState
+  int iters;
+  int start_iter;
+  double tolerance;
+  int pickless_step;
+  int check_on_pickless;
+  int rescan;
+  long long timeout_ns;
+};
+
+enum Mode { MODE_ASYNC = 0, MODE_SYNC = 1, MODE_SPLIT = 2 };
+
+// Persistent cooperative launch of all iterations; grid chosen from occupancy.
+cudaError_t launch_lpa(const LpaArgs &a, int slots, int mode, bool off64, cudaStream_t st, int *grid_out);
+// Per-slot-count instantiations (rak_lpa_s*.cu).
+template <int S>
+cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, cudaStream_t st, int *grid_out);
+
+// Plan and utility kernels (rak_kernels.cu).
+cudaError_t launch_validate(const void *off, bool off64, const uint32_t *tgt, int64_t n, int64_t m,
+                            unsigned int *bad, cudaStream_t st);
+cudaError_t launch_plan_keys(const void *off, bool off64, int64_t n, Layout ly, uint32_t *keys,
+                             uint32_t *vids, unsigned long long *hist, int nkeys, cudaStream_t st);
+cudaError_t plan_sort(uint32_t *keys_in, uint32_t *keys_out, uint32_t *vals_in, uint32_t *vals_out,
+                      int64_t n, int end_bit, void *temp, size_t *temp_bytes, cudaStream_t st);
+cudaError_t launch_init(uint32_t *vcom0, uint32_t *vcom1, const uint32_t *q, int64_t n, cudaStream_t st);
+cudaError_t launch_init_flags(uint8_t *aff0, uint8_t *aff1, const uint8_t *f, int64_t n, cudaStream_t st);
+cudaError_t launch_hub_degrees(const void *off, bool off64, const uint32_t *order, int64_t nhub,
+                               int64_t *deg, cudaStream_t st);
+cudaError_t launch_modularity(const void *off, bool off64, const uint32_t *tgt, const float *wt,
+                              int64_t n, const uint32_t *labels, double *ctot, double *sums,
+                              cudaStream_t st);
+
+}  // namespace rak

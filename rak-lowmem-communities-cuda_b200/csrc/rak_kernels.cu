@@ -1,0 +1,198 @@
+// rak_kernels.cu -- plan building, validation, initialisation and FP64 modularity kernels.
+#include <cub/device/device_radix_sort.cuh>
+
+#include "rak_device.cuh"
+#include "rak_internal.hpp"
+
+namespace rak {
+
+namespace {
+
+constexpr int TPB = 256;
+
+inline int grid_for(int64_t n, int per_thread = 1) {
+  int64_t g = (n + int64_t(TPB) * per_thread - 1) / (int64_t(TPB) * per_thread);
+  if (g < 1) g = 1;
+  if (g > 148 * 64) g = 148 * 64;
+  return int(g);
+}
+
+// CSR rules: offsets[0] == 0, non-decreasing, offsets[n] == m, every target < n.
+// Any violation sets *bad to 1 (a missing offset property) or 2 (a target out of range).
+template <class O>
+__global__ void k_validate(const O *off, const uint32_t *tgt, int64_t n, int64_t m, unsigned int *bad) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t u = tid; u < n; u += nt) {
+    const int64_t a = int64_t(off[u]), b = int64_t(off[u + 1]);
+    if (a > b || a < 0 || b > m) atomicOr(bad, 1u);
+  }
+  if (tid == 0 && (int64_t(off[0]) != 0 || int64_t(off[n]) != m)) atomicOr(bad, 1u);
+  for (int64_t e = tid; e < m; e += nt)
+    if (int64_t(tgt[e]) >= n) atomicOr(bad, 2u);
+}
+
+// Plan sort key of every vertex (plan_key) and a histogram of keys.
+template <class O>
+__global__ void k_plan_keys(const O *off, int64_t n, Layout ly, uint32_t *keys, uint32_t *vids,
+                            unsigned long long *hist, int nkeys) {
+  extern __shared__ unsigned int sh[];
+  for (int i = threadIdx.x; i < nkeys; i += blockDim.x) sh[i] = 0;
+  __syncthreads();
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t u = tid; u < n; u += nt) {
+    const uint32_t k = plan_key(int64_t(off[u + 1]) - int64_t(off[u]), ly);
+    keys[u] = k;
+    vids[u] = uint32_t(u);
+    atomicAdd(&sh[k], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nkeys; i += blockDim.x)
+    if (sh[i]) atomicAdd(hist + i, (unsigned long long)sh[i]);
+}
+
+template <class O>
+__global__ void k_hub_degrees(const O *off, const uint32_t *order, int64_t nhub, int64_t *deg) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t h = tid; h < nhub; h += nt) {
+    const uint32_t u = order[h];
+    deg[h] = int64_t(off[u + 1]) - int64_t(off[u]);
+  }
+}
+
+__global__ void k_init_labels(uint32_t *v0, uint32_t *v1, const uint32_t *q, int64_t n) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t u = tid; u < n; u += nt) {
+    const uint32_t c = q ? q[u] : uint32_t(u);
+    v0[u] = c;
+    if (v1) v1[u] = c;
+  }
+}
+
+__global__ void k_init_flags(uint8_t *f0, uint8_t *f1, const uint8_t *f, int64_t n) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t u = tid; u < n; u += nt) {
+    f0[u] = f ? (f[u] ? 1 : 0) : 1;
+    if (f1) f1[u] = 0;
+  }
+}
+
+// FP64 modularity terms (inc/properties.hxx:177-192): per vertex u with community c, the weight
+// of edges to its own community (summed into sums[0]), its total weight (into ctot[c]) and the
+// grand total (sums[1] = 2M). A second kernel sums ctot[c]^2 into sums[2].
+template <class O>
+__global__ void k_mod_vertex(const O *off, const uint32_t *tgt, const float *wt, int64_t n,
+                             const uint32_t *labels, double *ctot, double *sums) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5, nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  double in_acc = 0.0, tot_acc = 0.0;
+  for (int64_t u = w0; u < n; u += nw) {  // one warp per vertex
+    const uint32_t c = labels[u];
+    const int64_t eb = int64_t(off[u]), ee = int64_t(off[u + 1]);
+    double kin = 0.0, kt = 0.0;
+    for (int64_t e = eb + lane; e < ee; e += 32) {
+      const double w = wt ? double(wt[e]) : 1.0;
+      kt += w;
+      if (labels[tgt[e]] == c) kin += w;
+    }
+    kin = warp_sum(kin);
+    kt = warp_sum(kt);
+    if (lane == 0 && kt != 0.0) atomicAdd(ctot + c, kt);
+    in_acc += kin;
+    tot_acc += kt;
+  }
+  __shared__ double s_in[TPB / 32], s_tot[TPB / 32];
+  if (lane == 0) { s_in[threadIdx.x >> 5] = in_acc; s_tot[threadIdx.x >> 5] = tot_acc; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int i = 0; i < TPB / 32; ++i) { a += s_in[i]; b += s_tot[i]; }
+    atomicAdd(sums + 0, a);
+    atomicAdd(sums + 1, b);
+  }
+}
+
+__global__ void k_mod_square(const double *ctot, int64_t n, double *sums) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  double acc = 0.0;
+  for (int64_t c = tid; c < n; c += nt) acc += ctot[c] * ctot[c];
+  acc = warp_sum(acc);
+  __shared__ double s[TPB / 32];
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int i = 0; i < TPB / 32; ++i) a += s[i];
+    atomicAdd(sums + 2, a);
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_validate(const void *off, bool off64, const uint32_t *tgt, int64_t n, int64_t m,
+                            unsigned int *bad, cudaStream_t st) {
+  const int g = grid_for(n > m ? n : m, 4);
+  if (off64) k_validate<int64_t><<<g, TPB, 0, st>>>(static_cast<const int64_t *>(off), tgt, n, m, bad);
+  else k_validate<int32_t><<<g, TPB, 0, st>>>(static_cast<const int32_t *>(off), tgt, n, m, bad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_plan_keys(const void *off, bool off64, int64_t n, Layout ly, uint32_t *keys,
+                             uint32_t *vids, unsigned long long *hist, int nkeys, cudaStream_t st) {
+  const int g = grid_for(n, 8);
+  const size_t sh = size_t(nkeys) * sizeof(unsigned int);
+  if (off64) k_plan_keys<int64_t><<<g, TPB, sh, st>>>(static_cast<const int64_t *>(off), n, ly, keys, vids, hist, nkeys);
+  else k_plan_keys<int32_t><<<g, TPB, sh, st>>>(static_cast<const int32_t *>(off), n, ly, keys, vids, hist, nkeys);
+  return cudaGetLastError();
+}
+
+// Stable radix sort of (key, vertex id) pairs: vertices grouped by region, ascending id within
+// a key. With temp == nullptr only reports the temporary storage size.
+cudaError_t plan_sort(uint32_t *keys_in, uint32_t *keys_out, uint32_t *vals_in, uint32_t *vals_out,
+                      int64_t n, int end_bit, void *temp, size_t *temp_bytes, cudaStream_t st) {
+  return cub::DeviceRadixSort::SortPairs(temp, *temp_bytes, keys_in, keys_out, vals_in, vals_out, n, 0,
+                                         end_bit, st);
+}
+
+cudaError_t launch_hub_degrees(const void *off, bool off64, const uint32_t *order, int64_t nhub,
+                               int64_t *deg, cudaStream_t st) {
+  const int g = grid_for(nhub);
+  if (off64) k_hub_degrees<int64_t><<<g, TPB, 0, st>>>(static_cast<const int64_t *>(off), order, nhub, deg);
+  else k_hub_degrees<int32_t><<<g, TPB, 0, st>>>(static_cast<const int32_t *>(off), order, nhub, deg);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_init(uint32_t *vcom0, uint32_t *vcom1, const uint32_t *q, int64_t n, cudaStream_t st) {
+  k_init_labels<<<grid_for(n, 4), TPB, 0, st>>>(vcom0, vcom1, q, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_init_flags(uint8_t *aff0, uint8_t *aff1, const uint8_t *f, int64_t n, cudaStream_t st) {
+  k_init_flags<<<grid_for(n, 4), TPB, 0, st>>>(aff0, aff1, f, n);
+  return cudaGetLastError();
+}
+
+// ctot: n doubles (zeroed by the caller), sums: 3 doubles (zeroed by the caller) receive
+// [internal weight, total weight 2M, sum of squared community totals].
+cudaError_t launch_modularity(const void *off, bool off64, const uint32_t *tgt, const float *wt, int64_t n,
+                              const uint32_t *labels, double *ctot, double *sums, cudaStream_t st) {
+  const int g = grid_for(n * 32, 4);
+  if (off64) k_mod_vertex<int64_t><<<g, TPB, 0, st>>>(static_cast<const int64_t *>(off), tgt, wt, n, labels, ctot, sums);
+  else k_mod_vertex<int32_t><<<g, TPB, 0, st>>>(static_cast<const int32_t *>(off), tgt, wt, n, labels, ctot, sums);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_mod_square<<<grid_for(n, 4), TPB, 0, st>>>(ctot, n, sums);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lpa(const LpaArgs &a, int slots, int mode, bool off64, cudaStream_t st, int *grid_out) {
+  switch (slots) {
+    case 1: return launch_lpa_slots<1>(a, mode, off64, st, grid_out);
+    case 2: return launch_lpa_slots<2>(a, mode, off64, st, grid_out);
+    case 4: return launch_lpa_slots<4>(a, mode, off64, st, grid_out);
+    case 8: return launch_lpa_slots<8>(a, mode, off64, st, grid_out);
+    case 16: return launch_lpa_slots<16>(a, mode, off64, st, grid_out);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace rak

@@ -1,0 +1,450 @@
+// rak_lpa.cuh -- the persistent label-propagation kernel (all iterations in one cooperative
+// launch) for νMG-LPA (S >= 2 Misra-Gries slots) and νBM-LPA (S == 1).
+//
+// Reference path replaced: rakLowmemLoopCuU (inc/rakLowmemCuda.hxx:469-490) and the move kernels
+// it launches every iteration -- rakLowmemMgMoveIterationGroupCukU (:269-317),
+// rakLowmemMgMoveIterationBlockCukU (:362-419), rakLowmemBmMoveIterationThreadCukU (:138-161),
+// rakLowmemBmMoveIterationBlockCukU (:198-229) -- plus the per-iteration changed-count reset
+// (fillValueCuW, :477) and blocking read-back (:486). Here the changed count, the traversed-edge
+// count and the convergence test stay on the device; iterations are separated by a bounded grid
+// barrier instead of kernel launches and host round trips.
+//
+// Work is a static list of items over the plan's regions (rak_internal.hpp): warp w takes items
+// w, w + W, w + 2W, ... of every iteration, so each warp gets a similar mix of heavy and light
+// items. Sketches live in registers, one per lane.
+#pragma once
+#include "rak_device.cuh"
+#include "rak_internal.hpp"
+
+namespace rak {
+
+struct Counters {
+  unsigned long long edges;
+  unsigned int changed;
+  unsigned int processed;
+};
+
+template <class O>
+struct G_ {
+  const O *off;
+  const uint32_t *tgt;
+  const float *wt;
+};
+
+template <bool UNIT>
+__device__ __forceinline__ float edge_w(const float *wt, int64_t e) {
+  if constexpr (UNIT) return 1.0f;
+  else return __ldg(wt + e);
+}
+
+// Sequential sketch of edges e, e+st, ... < ee of u (self-loops skipped), four edges in flight.
+// Labels are read with plain loads: they change during the launch.
+template <int S, bool UNIT>
+__device__ __forceinline__ void scan_range(Sketch<S> &sk, uint32_t u, int64_t e, int64_t ee, int st,
+                                           const uint32_t *tgt, const float *wt, const uint32_t *vin) {
+  for (; e + 3 * int64_t(st) < ee; e += 4 * int64_t(st)) {
+    const uint32_t v0 = __ldg(tgt + e), v1 = __ldg(tgt + e + st), v2 = __ldg(tgt + e + 2 * st),
+                   v3 = __ldg(tgt + e + 3 * st);
+    const float w0 = edge_w<UNIT>(wt, e), w1 = edge_w<UNIT>(wt, e + st), w2 = edge_w<UNIT>(wt, e + 2 * st),
+                w3 = edge_w<UNIT>(wt, e + 3 * st);
+    const uint32_t c0 = vin[v0], c1 = vin[v1], c2 = vin[v2], c3 = vin[v3];
+    if (v0 != u) sk_acc(sk, c0, w0);
+    if (v1 != u) sk_acc(sk, c1, w1);
+    if (v2 != u) sk_acc(sk, c2, w2);
+    if (v3 != u) sk_acc(sk, c3, w3);
+  }
+  for (; e < ee; e += st) {
+    const uint32_t v = __ldg(tgt + e);
+    const float w = edge_w<UNIT>(wt, e);
+    const uint32_t c = vin[v];
+    if (v != u) sk_acc(sk, c, w);
+  }
+}
+
+// Exact weights of the sketch keys in edge order (inc/rakLowmem.hxx:154-162), one lane.
+template <int S, bool UNIT>
+__device__ __forceinline__ void rescan_range(Sketch<S> &sk, uint32_t u, int64_t e, int64_t ee,
+                                             const uint32_t *tgt, const float *wt, const uint32_t *vin) {
+#pragma unroll
+  for (int i = 0; i < S; ++i) sk.w[i] = 0.0f;
+  for (; e < ee; ++e) {
+    const uint32_t v = __ldg(tgt + e);
+    if (v == u) continue;
+    const uint32_t c = vin[v];
+    const float w = edge_w<UNIT>(wt, e);
+#pragma unroll
+    for (int i = 0; i < S; ++i)
+      if (sk.k[i] == c) sk.w[i] = __fadd_rn(sk.w[i], w);
+  }
+}
+
+// Marks neighbours e, e+st, ... < ee of a moved vertex u as affected (inc/rakCuda.hxx:95-103),
+// except u itself (the reference CPU loop clears u after marking, inc/rakLowmem.hxx:203,209).
+__device__ __forceinline__ void mark_range(uint32_t u, int64_t e, int64_t ee, int st, const uint32_t *tgt,
+                                           uint8_t *fout) {
+  for (; e + 3 * int64_t(st) < ee; e += 4 * int64_t(st)) {
+    const uint32_t v0 = __ldg(tgt + e), v1 = __ldg(tgt + e + st), v2 = __ldg(tgt + e + 2 * st),
+                   v3 = __ldg(tgt + e + 3 * st);
+    if (v0 != u) fout[v0] = 1;
+    if (v1 != u) fout[v1] = 1;
+    if (v2 != u) fout[v2] = 1;
+    if (v3 != u) fout[v3] = 1;
+  }
+  for (; e < ee; e += st) {
+    const uint32_t v = __ldg(tgt + e);
+    if (v != u) fout[v] = 1;
+  }
+}
+
+// Exact edge-order scan of u by the G lanes of one aligned group: lanes load G edges at a time,
+// then every lane applies them in order from shuffles, so all lanes hold the same sketch as a
+// single sequential scan would build (and, with rescan, the same exact weights).
+template <int S, bool UNIT>
+__device__ __forceinline__ void exact_group_scan(Sketch<S> &sk, uint32_t u, int64_t eb, int64_t ee, int G,
+                                                 int g, int s, bool rescan, const uint32_t *tgt,
+                                                 const float *wt, const uint32_t *vin) {
+  const unsigned gmask = G == 32 ? FULL : (((1u << G) - 1u) << (g * G));
+  for (int pass = 0; pass < (rescan ? 2 : 1); ++pass) {
+    if (pass == 1) {
+#pragma unroll
+      for (int i = 0; i < S; ++i) sk.w[i] = 0.0f;
+    }
+    for (int64_t base = eb; base < ee; base += G) {
+      const int64_t e = base + s;
+      uint32_t c = NONE;
+      float w = 0.0f;
+      int ok = 0;
+      if (e < ee) {
+        const uint32_t v = __ldg(tgt + e);
+        w = edge_w<UNIT>(wt, e);
+        c = vin[v];
+        ok = v != u;
+      }
+      const int cnt = int(ee - base < G ? ee - base : G);
+      for (int t = 0; t < cnt; ++t) {
+        const uint32_t ct = __shfl_sync(gmask, c, g * G + t);
+        const float wt_ = __shfl_sync(gmask, w, g * G + t);
+        const int okt = __shfl_sync(gmask, ok, g * G + t);
+        if (!okt) continue;
+        if (pass == 0) {
+          sk_acc(sk, ct, wt_);
+        } else {
+#pragma unroll
+          for (int i = 0; i < S; ++i)
+            if (sk.k[i] == ct) sk.w[i] = __fadd_rn(sk.w[i], wt_);
+        }
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ bool move_rule(float w, uint32_t c, uint32_t d, bool pickless) {
+  // inc/rakLowmem.hxx:203 (w>0 && c!=d) and inc/rakLowmemCuda.hxx:309 (pickless: no larger label)
+  return w > 0.0f && c != d && !(pickless && c > d);
+}
+
+// Region 6: one lane per vertex.
+template <int S, int MODE, class O, bool UNIT>
+__device__ __forceinline__ void lane_item(const LpaArgs &a, const Regions &rg, const G_<O> &g, int64_t local, bool pickless,
+                                          const uint32_t *vin, uint32_t *vout, uint8_t *fin, uint8_t *fout,
+                                          Counters &cnt) {
+  const int lane = threadIdx.x & 31;
+  const int64_t idx = local * 32 + lane;
+  if (idx >= rg.vcount[REG_LANE]) return;
+  const uint32_t u = __ldg(a.order + rg.vbegin[REG_LANE] + idx);
+  const uint32_t d = vin[u];
+  if (!fin[u]) {
+    if constexpr (MODE != MODE_ASYNC) vout[u] = d;
+    return;
+  }
+  const int64_t eb = int64_t(__ldg(g.off + u)), ee = int64_t(__ldg(g.off + u + 1));
+  Sketch<S> sk;
+  sk_clear(sk);
+  scan_range<S, UNIT>(sk, u, eb, ee, 1, g.tgt, g.wt, vin);
+  if constexpr (MODE == MODE_SYNC && S > 1)
+    if (a.rescan) rescan_range<S, UNIT>(sk, u, eb, ee, g.tgt, g.wt, vin);
+  uint32_t c;
+  float w;
+  sk_choose(sk, c, w);
+  const bool moved = move_rule(w, c, d, pickless);
+  cnt.processed += 1;
+  cnt.edges += (unsigned long long)(ee - eb);
+  if constexpr (MODE == MODE_ASYNC) {
+    fin[u] = 0;
+    if (moved) vout[u] = c;
+  } else {
+    vout[u] = moved ? c : d;
+  }
+  if (moved) {
+    cnt.changed += 1;
+    mark_range(u, eb, ee, 1, g.tgt, fout);
+  }
+}
+
+// Regions 1..5: aligned groups of G lanes per vertex.
+template <int S, int MODE, class O, bool UNIT>
+__device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, const G_<O> &g, int r, int64_t local, bool pickless,
+                                           const uint32_t *vin, uint32_t *vout, uint8_t *fin, uint8_t *fout,
+                                           Counters &cnt) {
+  const int G = region_group(r);
+  const int lane = threadIdx.x & 31, grp = lane / G, s = lane & (G - 1);
+  const int64_t idx = local * (32 / G) + grp;
+  const bool valid = idx < rg.vcount[r];
+  uint32_t u = 0, d = 0;
+  int64_t eb = 0, ee = 0;
+  bool active = false;
+  if (valid) {
+    u = __ldg(a.order + rg.vbegin[r] + idx);
+    d = vin[u];
+    active = fin[u] != 0;
+    if (active) { eb = int64_t(__ldg(g.off + u)); ee = int64_t(__ldg(g.off + u + 1)); }
+  }
+  Sketch<S> sk;
+  sk_clear(sk);
+  if constexpr (MODE == MODE_SYNC) {
+    if (active) exact_group_scan<S, UNIT>(sk, u, eb, ee, G, grp, s, S > 1 && a.rescan, g.tgt, g.wt, vin);
+  } else {
+    if (active) scan_range<S, UNIT>(sk, u, eb + s, ee, G, g.tgt, g.wt, vin);
+    sk_tree(sk, G);
+  }
+  uint32_t c;
+  float w;
+  sk_choose(sk, c, w);
+  bool moved = active && move_rule(w, c, d, pickless);
+  moved = __shfl_sync(FULL, moved, grp * G);
+  if (s == 0 && valid) {
+    if (active) { cnt.processed += 1; cnt.edges += (unsigned long long)(ee - eb); }
+    if constexpr (MODE == MODE_ASYNC) {
+      if (active) fin[u] = 0;
+      if (moved) vout[u] = c;
+    } else {
+      vout[u] = moved ? c : d;
+    }
+    if (moved) cnt.changed += 1;
+  }
+  if (moved) mark_range(u, eb + s, ee, G, g.tgt, fout);
+}
+
+// Region 0: one chunk of a split vertex per item. In the synchronous exact mode chunk 0's warp
+// scans the whole vertex in edge order and the other chunks do nothing. Otherwise each chunk's
+// warp builds a partial sketch (lane-strided, tree-merged), stores it, and the last chunk to
+// arrive merges all partial sketches in a fixed order and makes the move; its neighbours are
+// marked in a second phase after the iteration's barrier.
+template <int S, int MODE, class O, bool UNIT>
+__device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, const G_<O> &g, int64_t local, int it, bool pickless,
+                                         const uint32_t *vin, uint32_t *vout, uint8_t *fin, uint8_t *fout,
+                                         Counters &cnt) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t h = __ldg(a.chunk_hub + local);
+  const int64_t first = __ldg(a.hub_first + h), nch = __ldg(a.hub_first + h + 1) - first, j = local - first;
+  const uint32_t u = __ldg(a.order + rg.vbegin[REG_HUB] + h);
+  const int64_t eb = int64_t(__ldg(g.off + u)), ee = int64_t(__ldg(g.off + u + 1));
+  if constexpr (MODE == MODE_SYNC) {
+    if (j != 0) return;
+    const uint32_t d = vin[u];
+    const bool active = fin[u] != 0;
+    Sketch<S> sk;
+    sk_clear(sk);
+    if (active) exact_group_scan<S, UNIT>(sk, u, eb, ee, 32, 0, lane, S > 1 && a.rescan, g.tgt, g.wt, vin);
+    uint32_t c;
+    float w;
+    sk_choose(sk, c, w);
+    const bool moved = active && move_rule(w, c, d, pickless);
+    if (lane == 0) {
+      vout[u] = moved ? c : d;
+      if (active) { cnt.processed += 1; cnt.edges += (unsigned long long)(ee - eb); }
+      if (moved) cnt.changed += 1;
+    }
+    if (moved) mark_range(u, eb + lane, ee, 32, g.tgt, fout);
+    return;
+  } else {
+    bool active;
+    if constexpr (MODE == MODE_SPLIT) {
+      active = fin[u] != 0;
+    } else {
+      // All chunks of u agree on whether u is processed this iteration: the first chunk to get
+      // here decides from u's flag (and clears it); the others read the decision.
+      unsigned int dec = 0;
+      if (lane == 0) {
+        const unsigned int tag = unsigned(it + 1);
+        unsigned int cur = *(volatile unsigned int *)(a.hub_claim + h);
+        if ((cur >> 1) != tag) {
+          const unsigned int want = (tag << 1) | (*(volatile uint8_t *)(fin + u) ? 1u : 0u);
+          const unsigned int prev = atomicCAS(a.hub_claim + h, cur, want);
+          if (prev == cur) {
+            cur = want;
+            if (want & 1u) fin[u] = 0;
+          } else {
+            cur = prev;
+          }
+        }
+        dec = cur & 1u;
+      }
+      active = __shfl_sync(FULL, dec, 0) != 0;
+    }
+    Sketch<S> sk;
+    sk_clear(sk);
+    const int64_t cb = eb + j * a.hub_chunk, ce = cb + a.hub_chunk < ee ? cb + a.hub_chunk : ee;
+    if (active) scan_range<S, UNIT>(sk, u, cb + lane, ce, 32, g.tgt, g.wt, vin);
+    sk_tree(sk, 32);
+    unsigned int last = 0;
+    if (lane == 0) {
+      if (active) {
+        cnt.edges += (unsigned long long)(ce - cb);
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+          a.sk_keys[local * S + i] = sk.k[i];
+          a.sk_wts[local * S + i] = sk.w[i];
+        }
+      }
+      __threadfence();
+      last = atomicAdd(a.hub_arrive + h, 1u) == unsigned(nch - 1);
+    }
+    last = __shfl_sync(FULL, last, 0);
+    if (!last) return;
+    __threadfence();
+    if (lane == 0) a.hub_arrive[h] = 0;
+    const uint32_t d = vin[u];
+    if (!active) {
+      if (MODE != MODE_ASYNC && lane == 0) vout[u] = d;
+      return;
+    }
+    Sketch<S> acc;
+    sk_clear(acc);
+    for (int64_t jj = lane; jj < nch; jj += 32) {
+      uint32_t bk[S];
+      float bw[S];
+#pragma unroll
+      for (int i = 0; i < S; ++i) {
+        bk[i] = __ldcg(a.sk_keys + (first + jj) * S + i);
+        bw[i] = __ldcg(a.sk_wts + (first + jj) * S + i);
+      }
+      sk_merge(acc, bk, bw);
+    }
+    sk_tree(acc, 32);
+    if (lane == 0) {
+      uint32_t c;
+      float w;
+      sk_choose(acc, c, w);
+      const bool moved = move_rule(w, c, d, pickless);
+      cnt.processed += 1;
+      if constexpr (MODE == MODE_ASYNC) {
+        if (moved) vout[u] = c;
+      } else {
+        vout[u] = moved ? c : d;
+      }
+      if (moved) {
+        cnt.changed += 1;
+        a.hub_moved[h] = it;
+        atomicAdd(a.stats + 4 * it + 3, 1ull);
+      }
+    }
+  }
+}
+
+template <int S, int MODE, class O, bool UNIT>
+__global__ void __launch_bounds__(256, 2) lpa_run(const LpaArgs a) {
+  const G_<O> g{static_cast<const O *>(a.off), a.tgt, a.wt};
+  RunState *rs = static_cast<RunState *>(a.rs);
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  __shared__ unsigned long long blk[3];
+  __shared__ Regions rg;  // copied once: indexed by region at run time
+  if (threadIdx.x == 0) rg = a.rg;
+  unsigned int epoch = 0;
+  for (int it = 0; it < a.iters; ++it) {
+    if (threadIdx.x < 3) blk[threadIdx.x] = 0;
+    __syncthreads();
+    const int l = a.start_iter + it;
+    const bool pickless = a.pickless_step > 0 && l % a.pickless_step == 0;
+    const bool odd = MODE != MODE_ASYNC && (it & 1);
+    const uint32_t *vin = odd ? a.vcom1 : a.vcom0;
+    uint32_t *vout = MODE == MODE_ASYNC ? a.vcom0 : (odd ? a.vcom0 : a.vcom1);
+    uint8_t *fin = odd ? a.aff1 : a.aff0;
+    uint8_t *fout = MODE == MODE_ASYNC ? a.aff0 : (odd ? a.aff0 : a.aff1);
+    Counters cnt{0, 0, 0};
+    const int64_t total = rg.ibegin[NREG];
+    for (int64_t item = gw; item < total; item += nw) {
+      int r = 0;
+      while (item >= rg.ibegin[r + 1]) ++r;
+      const int64_t local = item - rg.ibegin[r];
+      if (r == REG_HUB) hub_item<S, MODE, O, UNIT>(a, rg, g, local, it, pickless, vin, vout, fin, fout, cnt);
+      else if (r == REG_LANE) lane_item<S, MODE, O, UNIT>(a, rg, g, local, pickless, vin, vout, fin, fout, cnt);
+      else group_item<S, MODE, O, UNIT>(a, rg, g, r, local, pickless, vin, vout, fin, fout, cnt);
+    }
+    const unsigned long long ch = warp_sum((unsigned long long)cnt.changed);
+    const unsigned long long ed = warp_sum(cnt.edges);
+    const unsigned long long pr = warp_sum((unsigned long long)cnt.processed);
+    if (lane == 0) {
+      if (ch) atomicAdd(&blk[0], ch);
+      if (ed) atomicAdd(&blk[1], ed);
+      if (pr) atomicAdd(&blk[2], pr);
+    }
+    __syncthreads();
+    if (threadIdx.x < 3 && blk[threadIdx.x]) atomicAdd(a.stats + 4 * it + threadIdx.x, blk[threadIdx.x]);
+    if (!grid_barrier(rs, ++epoch, a.timeout_ns)) return;
+    const unsigned long long changed = __ldcg(a.stats + 4 * it);
+    const bool test = !pickless || a.check_on_pickless;
+    const bool done = it + 1 >= a.iters || (test && double(changed) / double(a.n) <= a.tolerance);
+    // The synchronous split mode completes the next flags even on the last iteration, so a
+    // single step returns them whole.
+    if (MODE != MODE_SYNC && (!done || MODE == MODE_SPLIT) && a.nchunks > 0 && __ldcg(a.stats + 4 * it + 3) > 0) {
+      // Second phase: neighbours of split vertices that moved this iteration.
+      for (int64_t i = gw; i < a.nchunks; i += nw) {
+        const uint32_t h = __ldg(a.chunk_hub + i);
+        if (__ldcg(a.hub_moved + h) != it) continue;
+        const uint32_t u = __ldg(a.order + rg.vbegin[REG_HUB] + h);
+        const int64_t eb = int64_t(__ldg(g.off + u)), ee = int64_t(__ldg(g.off + u + 1));
+        const int64_t j = i - __ldg(a.hub_first + h);
+        const int64_t cb = eb + j * a.hub_chunk, ce = cb + a.hub_chunk < ee ? cb + a.hub_chunk : ee;
+        mark_range(u, cb + lane, ce, 32, g.tgt, fout);
+      }
+    }
+    if (done) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) rs->iterations = unsigned(it + 1);
+      return;
+    }
+    if constexpr (MODE != MODE_ASYNC) {
+      // The flags just read become next iteration's output: clear them.
+      const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+      uint4 *f4 = reinterpret_cast<uint4 *>(fin);
+      const int64_t n16 = a.n >> 4;
+      for (int64_t i = tid; i < n16; i += nt) f4[i] = make_uint4(0, 0, 0, 0);
+      for (int64_t i = (n16 << 4) + tid; i < a.n; i += nt) fin[i] = 0;
+      if (!grid_barrier(rs, ++epoch, a.timeout_ns)) return;
+    }
+  }
+}
+
+template <int S>
+cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, cudaStream_t st, int *grid_out) {
+  const void *fn = nullptr;
+  const bool unit = a.wt == nullptr;
+#define RAK_PICK(M, O, U) \
+  if (mode == M && off64 == (sizeof(O) == 8) && unit == U) fn = reinterpret_cast<const void *>(&lpa_run<S, M, O, U>);
+  RAK_PICK(MODE_ASYNC, int32_t, false) RAK_PICK(MODE_ASYNC, int32_t, true)
+  RAK_PICK(MODE_ASYNC, int64_t, false) RAK_PICK(MODE_ASYNC, int64_t, true)
+  RAK_PICK(MODE_SYNC, int32_t, false) RAK_PICK(MODE_SYNC, int32_t, true)
+  RAK_PICK(MODE_SYNC, int64_t, false) RAK_PICK(MODE_SYNC, int64_t, true)
+  RAK_PICK(MODE_SPLIT, int32_t, false) RAK_PICK(MODE_SPLIT, int32_t, true)
+  RAK_PICK(MODE_SPLIT, int64_t, false) RAK_PICK(MODE_SPLIT, int64_t, true)
+#undef RAK_PICK
+  if (!fn) return cudaErrorInvalidValue;
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0)) != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  const int64_t warps_needed = a.rg.ibegin[NREG] > 0 ? a.rg.ibegin[NREG] : 1;
+  int64_t grid = int64_t(per_sm) * sms;
+  const int64_t want = (warps_needed + 7) / 8;
+  if (want < grid) grid = want;
+  if (grid < 1) grid = 1;
+  if (grid_out) *grid_out = int(grid);
+  void *args[] = {const_cast<LpaArgs *>(&a)};
+  return cudaLaunchCooperativeKernel(fn, dim3(unsigned(grid)), dim3(256), args, 0, st);
+}
+
+}  // namespace rak

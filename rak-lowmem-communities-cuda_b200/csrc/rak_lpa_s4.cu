@@ -1,0 +1,6 @@
+// Instantiates the persistent LPA kernel for 4 sketch slot(s) (separate unit: parallel build).
+#include "rak_lpa.cuh"
+
+namespace rak {
+template cudaError_t launch_lpa_slots<4>(const LpaArgs &, int, bool, cudaStream_t, int *);
+}

@@ -1,0 +1,356 @@
+"""Python binding (ctypes) of librak_lowmem.so, the B200 memory-efficient label propagation library.
+
+Mirrors the reference's call shape: ``rakLowmemStaticCuda<SLOTS>(x, o) -> RakResult`` becomes
+``Context.lowmem(graph, q=None, options) -> (membership, result)`` with the same option names
+(repeat, tolerance, max_iterations) and result fields (iterations, time_ms, marking_time_ms,
+initialization_time_ms, memory_gb). The native library is required: importing this module raises
+if ``librak_lowmem.so`` is missing; there is no CPU fallback.
+
+Host graphs are numpy arrays; device graphs are torch CUDA tensors (torch only provides device
+memory and streams here).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librak_lowmem.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"{LIB_PATH} is missing: build it with `make -C {_HERE}` (or __graft_entry__.build())")
+_lib = C.CDLL(LIB_PATH)
+
+HOST, DEVICE = 0, 1
+MODE_ASYNC, MODE_SYNC, MODE_SYNC_SPLIT = 0, 1, 2
+STATUS = {0: "ok", 1: "invalid argument", 2: "invalid CSR", 3: "out of memory", 4: "CUDA error",
+          5: "timeout", 6: "no device", 7: "unsupported", 8: "busy"}
+
+
+class rak_csr(C.Structure):
+    _fields_ = [("n", C.c_int64), ("m", C.c_int64), ("offset_bits", C.c_int32), ("location", C.c_int32),
+                ("offsets", C.c_void_p), ("targets", C.c_void_p), ("weights", C.c_void_p)]
+
+
+class rak_options(C.Structure):
+    _fields_ = [("repeat", C.c_int32), ("tolerance", C.c_double), ("max_iterations", C.c_int32),
+                ("slots", C.c_int32), ("mode", C.c_int32), ("rescan", C.c_int32),
+                ("pickless_step", C.c_int32), ("check_on_pickless", C.c_int32), ("lane_max", C.c_int32),
+                ("hub_min", C.c_int32), ("hub_chunk", C.c_int32), ("validate", C.c_int32),
+                ("compute_modularity", C.c_int32), ("start_iteration", C.c_int32),
+                ("initial_flags", C.c_void_p), ("reserved", C.c_int64 * 8)]
+
+
+class rak_result(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("time_ms", C.c_float), ("marking_time_ms", C.c_float),
+                ("initialization_time_ms", C.c_float), ("memory_gb", C.c_float), ("plan_ms", C.c_float),
+                ("h2d_ms", C.c_float), ("d2h_ms", C.c_float), ("peak_device_bytes", C.c_uint64),
+                ("traversed_edges", C.c_uint64), ("processed_vertices", C.c_uint64),
+                ("changed_last", C.c_uint64), ("modularity", C.c_double)]
+
+
+class rak_host_csr(C.Structure):
+    _fields_ = [("n", C.c_int64), ("m", C.c_int64), ("offsets", C.c_void_p), ("targets", C.c_void_p),
+                ("weights", C.c_void_p), ("truth", C.c_void_p)]
+
+
+def _sig(name, res, *args):
+    f = getattr(_lib, name)
+    f.restype = res
+    f.argtypes = list(args)
+    return f
+
+
+P = C.c_void_p
+_sig("rak_abi_version", C.c_int)
+_sig("rak_status_string", C.c_char_p, C.c_int)
+_sig("rak_options_default", None, C.POINTER(rak_options))
+_sig("rak_ctx_create", C.c_int, C.c_int, C.POINTER(P))
+_sig("rak_ctx_destroy", C.c_int, P)
+_sig("rak_ctx_set_stream", C.c_int, P, P)
+_sig("rak_ctx_last_error", C.c_char_p, P)
+_sig("rak_lowmem_cuda", C.c_int, P, C.POINTER(rak_csr), P, C.POINTER(rak_options), P, C.POINTER(rak_result))
+_sig("rak_graph_create", C.c_int, P, C.POINTER(rak_csr), C.POINTER(rak_options), C.POINTER(P))
+_sig("rak_graph_destroy", C.c_int, P)
+_sig("rak_graph_device_bytes", C.c_uint64, P)
+_sig("rak_graph_run", C.c_int, P, P, P, C.POINTER(rak_options), P, C.POINTER(rak_result))
+_sig("rak_graph_step", C.c_int, P, P, C.POINTER(rak_options), C.c_int, P, P, P, P, C.POINTER(C.c_uint64))
+_sig("rak_modularity_f64", C.c_int, P, C.POINTER(rak_csr), P, C.POINTER(C.c_double))
+_sig("rak_gen_rmat", C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64,
+     C.c_float, C.c_float, C.c_int, C.POINTER(rak_host_csr))
+_sig("rak_gen_sbm", C.c_int, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_uint64, C.c_int,
+     C.POINTER(rak_host_csr))
+_sig("rak_gen_lattice", C.c_int, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_uint64, C.c_int,
+     C.POINTER(rak_host_csr))
+_sig("rak_host_csr_free", None, C.POINTER(rak_host_csr))
+_sig("rak_csr_validate_host", C.c_int, C.POINTER(rak_csr))
+_sig("rak_plan_summary_host", C.c_int, C.POINTER(rak_csr), C.POINTER(rak_options), C.POINTER(C.c_int64),
+     C.POINTER(C.c_int64))
+
+
+class RakError(RuntimeError):
+    def __init__(self, status: int, msg: str = ""):
+        self.status = status
+        super().__init__(f"{STATUS.get(status, status)}: {msg}" if msg else STATUS.get(status, str(status)))
+
+
+def abi_version() -> int:
+    return _lib.rak_abi_version()
+
+
+def options(**kw) -> rak_options:
+    """Defaults of rak_options_default, overridden by keyword (field names of rak_options)."""
+    o = rak_options()
+    _lib.rak_options_default(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise TypeError(f"unknown option {k}")
+        setattr(o, k, v)
+    return o
+
+
+@dataclass
+class Result:
+    """RakResult<K> fields plus this library's counters."""
+    iterations: int
+    time_ms: float
+    marking_time_ms: float
+    initialization_time_ms: float
+    memory_gb: float
+    plan_ms: float
+    h2d_ms: float
+    d2h_ms: float
+    peak_device_bytes: int
+    traversed_edges: int
+    processed_vertices: int
+    changed_last: int
+    modularity: float
+
+    @staticmethod
+    def of(r: rak_result) -> "Result":
+        return Result(*[getattr(r, f[0]) for f in rak_result._fields_])
+
+
+class HostGraph:
+    """A host CSR: offsets (int32 or int64, n+1), targets (uint32, m), weights (float32 or None)."""
+
+    def __init__(self, offsets, targets, weights=None, truth=None, _owner=None):
+        self.offsets = offsets
+        self.targets = targets
+        self.weights = weights
+        self.truth = truth
+        self._owner = _owner
+        self.n = len(offsets) - 1
+        self.m = int(offsets[-1]) if self.n >= 0 else 0
+
+    def csr(self) -> rak_csr:
+        return rak_csr(self.n, self.m, 64 if self.offsets.dtype == np.int64 else 32, HOST,
+                       self.offsets.ctypes.data, self.targets.ctypes.data if self.m else None,
+                       self.weights.ctypes.data if self.weights is not None else None)
+
+    def with_offsets32(self) -> "HostGraph":
+        return HostGraph(self.offsets.astype(np.int32), self.targets, self.weights, self.truth, self._owner)
+
+    def degrees(self) -> np.ndarray:
+        return np.diff(self.offsets.astype(np.int64))
+
+
+class _Owned:
+    def __init__(self, h: rak_host_csr):
+        self.h = h
+
+    def __del__(self):
+        _lib.rak_host_csr_free(C.byref(self.h))
+
+
+def _wrap_host(h: rak_host_csr) -> HostGraph:
+    owner = _Owned(h)
+    n, m = h.n, h.m
+
+    def arr(ptr, ctype, count, dtype):
+        if not ptr or count == 0:
+            return np.zeros(count, dtype=dtype)
+        return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), shape=(count,)).view(dtype)
+
+    off = arr(h.offsets, C.c_int64, n + 1, np.int64)
+    tgt = arr(h.targets, C.c_uint32, m, np.uint32)
+    wt = arr(h.weights, C.c_float, m, np.float32) if h.weights else None
+    truth = arr(h.truth, C.c_uint32, n, np.uint32) if h.truth else None
+    return HostGraph(off, tgt, wt, truth, owner)
+
+
+def _check(st: int, ctx=None):
+    if st != 0:
+        msg = _lib.rak_ctx_last_error(ctx).decode() if ctx else ""
+        raise RakError(st, msg)
+
+
+def gen_rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=42, w_lo=1.0, w_hi=1.0, threads=0) -> HostGraph:
+    h = rak_host_csr()
+    _check(_lib.rak_gen_rmat(scale, edge_factor, a, b, c, seed, w_lo, w_hi, threads, C.byref(h)))
+    return _wrap_host(h)
+
+
+def gen_sbm(n, k, avg_degree=16.0, in_out_ratio=20.0, seed=42, threads=0) -> HostGraph:
+    h = rak_host_csr()
+    _check(_lib.rak_gen_sbm(n, k, avg_degree, in_out_ratio, seed, threads, C.byref(h)))
+    return _wrap_host(h)
+
+
+def gen_lattice(width, height, p_delete=0.05, shortcut_frac=0.01, seed=42, threads=0) -> HostGraph:
+    h = rak_host_csr()
+    _check(_lib.rak_gen_lattice(width, height, p_delete, shortcut_frac, seed, threads, C.byref(h)))
+    return _wrap_host(h)
+
+
+def validate_host(g: HostGraph) -> int:
+    c = g.csr()
+    return _lib.rak_csr_validate_host(C.byref(c))
+
+
+def plan_summary(g: HostGraph, **opts):
+    c = g.csr()
+    counts = (C.c_int64 * 8)()
+    chunks = C.c_int64(0)
+    o = options(**opts)
+    _check(_lib.rak_plan_summary_host(C.byref(c), C.byref(o), counts, C.byref(chunks)))
+    return list(counts), chunks.value
+
+
+def _ptr(t) -> Optional[int]:
+    return None if t is None else t.data_ptr()
+
+
+def device_csr(offsets, targets, weights=None) -> rak_csr:
+    """rak_csr over torch CUDA tensors (offsets int32/int64, targets int32 holding uint32 ids)."""
+    import torch
+    n = offsets.numel() - 1
+    return rak_csr(n, targets.numel(), 64 if offsets.dtype == torch.int64 else 32, DEVICE,
+                   offsets.data_ptr(), _ptr(targets) if targets.numel() else None, _ptr(weights))
+
+
+class Context:
+    """A device context (rak_ctx): one device, one stream."""
+
+    def __init__(self, device: int = 0):
+        self._c = P()
+        _check(_lib.rak_ctx_create(device, C.byref(self._c)))
+
+    def close(self):
+        if self._c:
+            _lib.rak_ctx_destroy(self._c)
+            self._c = P()
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._c
+
+    def set_stream(self, stream_ptr: Optional[int]):
+        _check(_lib.rak_ctx_set_stream(self._c, stream_ptr), self._c)
+
+    def last_error(self) -> str:
+        return _lib.rak_ctx_last_error(self._c).decode()
+
+    def lowmem(self, g: HostGraph, q: Optional[np.ndarray] = None, flags: Optional[np.ndarray] = None,
+               **opts):
+        """rakLowmemStaticCuda<slots>(x, o) on a host graph: (membership, Result)."""
+        o = options(**opts)
+        if flags is not None:
+            flags = np.ascontiguousarray(flags, dtype=np.uint8)
+            o.initial_flags = flags.ctypes.data
+        c = g.csr()
+        out = np.empty(g.n, dtype=np.uint32)
+        r = rak_result()
+        qp = None
+        if q is not None:
+            q = np.ascontiguousarray(q, dtype=np.uint32)
+            qp = q.ctypes.data
+        _check(_lib.rak_lowmem_cuda(self._c, C.byref(c), qp, C.byref(o), out.ctypes.data, C.byref(r)), self._c)
+        return out, Result.of(r)
+
+    def lowmem_device(self, csr: rak_csr, membership, q=None, **opts):
+        """The same on a device-located csr; membership (and q) are torch CUDA tensors."""
+        o = options(**opts)
+        r = rak_result()
+        _check(_lib.rak_lowmem_cuda(self._c, C.byref(csr), _ptr(q), C.byref(o), membership.data_ptr(),
+                                    C.byref(r)), self._c)
+        return Result.of(r)
+
+    def modularity(self, csr_or_graph, membership) -> float:
+        """FP64 modularity on the device (rak_modularity_f64)."""
+        if isinstance(csr_or_graph, HostGraph):
+            c = csr_or_graph.csr()
+            membership = np.ascontiguousarray(membership, dtype=np.uint32)
+            mp = membership.ctypes.data
+        else:
+            c = csr_or_graph
+            mp = membership.data_ptr()
+        q = C.c_double(math.nan)
+        _check(_lib.rak_modularity_f64(self._c, C.byref(c), mp, C.byref(q)), self._c)
+        return q.value
+
+
+class ResidentGraph:
+    """A device-resident graph with its plan (rak_graph)."""
+
+    def __init__(self, ctx: Context, csr_or_graph, **opts):
+        self.ctx = ctx
+        self._keep = csr_or_graph
+        c = csr_or_graph.csr() if isinstance(csr_or_graph, HostGraph) else csr_or_graph
+        self.n = c.n
+        self._g = P()
+        o = options(**opts)
+        _check(_lib.rak_graph_create(ctx.handle, C.byref(c), C.byref(o), C.byref(self._g)), ctx.handle)
+
+    def close(self):
+        if self._g:
+            _lib.rak_graph_destroy(self._g)
+            self._g = P()
+
+    def __del__(self):
+        self.close()
+
+    def device_bytes(self) -> int:
+        return _lib.rak_graph_device_bytes(self._g)
+
+    def run(self, membership, q=None, **opts) -> Result:
+        o = options(**opts)
+        r = rak_result()
+        _check(_lib.rak_graph_run(self.ctx.handle, self._g, _ptr(q), C.byref(o), membership.data_ptr(),
+                                  C.byref(r)), self.ctx.handle)
+        return Result.of(r)
+
+    def step(self, iteration, vcom_prev, aff_prev, vcom_next, aff_next, **opts) -> int:
+        o = options(**opts)
+        ch = C.c_uint64(0)
+        _check(_lib.rak_graph_step(self.ctx.handle, self._g, C.byref(o), iteration, vcom_prev.data_ptr(),
+                                   aff_prev.data_ptr(), vcom_next.data_ptr(), aff_next.data_ptr(),
+                                   C.byref(ch)), self.ctx.handle)
+        return ch.value
+
+
+def write_rakcsr(path: str, g: HostGraph):
+    """Binary CSR file: b"RAKCSR01", int64 n, int64 m, int32 has_weights, int64 offsets[n+1],
+    uint32 targets[m], float32 weights[m] (if present)."""
+    with open(path, "wb") as f:
+        f.write(b"RAKCSR01")
+        f.write(np.array([g.n, g.m], dtype=np.int64).tobytes())
+        f.write(np.array([1 if g.weights is not None else 0], dtype=np.int32).tobytes())
+        f.write(g.offsets.astype(np.int64).tobytes())
+        f.write(g.targets.astype(np.uint32).tobytes())
+        if g.weights is not None:
+            f.write(g.weights.astype(np.float32).tobytes())
