@@ -429,13 +429,14 @@ rak_status modularity_dev(rak_ctx *ctx, const void *off, bool off64, const uint3
                           const uint32_t *labels, Tracker *tr, double *q) {
   DevBuf ctot, sums;
   RAK_TRY(ctx, ctot.alloc(size_t(std::max<int64_t>(n, 1)) * 8, tr));
-  RAK_TRY(ctx, sums.alloc(3 * 8, tr));
+  RAK_TRY(ctx, sums.alloc(4 * 8, tr));
   RAK_TRY(ctx, cudaMemsetAsync(ctot.p, 0, ctot.bytes, ctx->stream));
   RAK_TRY(ctx, cudaMemsetAsync(sums.p, 0, sums.bytes, ctx->stream));
-  double h[3] = {0, 0, 0};
+  double h[4] = {0, 0, 0, 0};
   if (n > 0) RAK_TRY(ctx, rak::launch_modularity(off, off64, tgt, wt, n, labels, ctot.as<double>(), sums.as<double>(), ctx->stream));
   RAK_TRY(ctx, cudaMemcpyAsync(h, sums.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
   RAK_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (h[3] > 0) { set_err(ctx, "membership holds labels >= n"); return RAK_ERR_INVALID_ARGUMENT; }
   *q = h[1] > 0 ? h[0] / h[1] - h[2] / (h[1] * h[1]) : 0.0;
   return RAK_OK;
 }
@@ -663,8 +664,18 @@ rak_status rak_modularity_f64(rak_ctx *ctx, const rak_csr *g, const uint32_t *me
   if (!ctx || !g || !membership || !q) return RAK_ERR_INVALID_ARGUMENT;
   RAK_CHECK(check_csr_shape(ctx, g));
   RAK_TRY(ctx, cudaSetDevice(ctx->device));
-  if (g->location == RAK_DEVICE)
+  if (g->location == RAK_DEVICE) {
+    DevBuf bad;
+    unsigned int hbad = 0;
+    RAK_TRY(ctx, bad.alloc(4, nullptr));
+    RAK_TRY(ctx, cudaMemsetAsync(bad.p, 0, 4, ctx->stream));
+    RAK_TRY(ctx, rak::launch_validate(g->offsets, g->offset_bits == 64, g->targets, g->n, g->m, bad.as<unsigned int>(), ctx->stream));
+    RAK_TRY(ctx, cudaMemcpyAsync(&hbad, bad.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    RAK_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (hbad) { set_err(ctx, "invalid CSR (device check)"); return RAK_ERR_INVALID_CSR; }
     return modularity_dev(ctx, g->offsets, g->offset_bits == 64, g->targets, g->weights, g->n, membership, nullptr, q);
+  }
+  if (rak_csr_validate_host(g) != RAK_OK) { set_err(ctx, "invalid CSR (host check)"); return RAK_ERR_INVALID_CSR; }
   const int64_t n = g->n, m = g->m;
   const size_t ob = size_t(n + 1) * (g->offset_bits == 64 ? 8 : 4);
   DevBuf off, tgt, wt, lab;

@@ -87,6 +87,10 @@ __global__ void k_mod_vertex(const O *off, const uint32_t *tgt, const float *wt,
   double in_acc = 0.0, tot_acc = 0.0;
   for (int64_t u = w0; u < n; u += nw) {  // one warp per vertex
     const uint32_t c = labels[u];
+    if (int64_t(c) >= n) {  // not a vertex id: counted, and the host reports the error
+      if (lane == 0) atomicAdd(sums + 3, 1.0);
+      continue;
+    }
     const int64_t eb = int64_t(off[u]), ee = int64_t(off[u + 1]);
     double kin = 0.0, kt = 0.0;
     for (int64_t e = eb + lane; e < ee; e += 32) {
@@ -171,8 +175,8 @@ cudaError_t launch_init_flags(uint8_t *aff0, uint8_t *aff1, const uint8_t *f, in
   return cudaGetLastError();
 }
 
-// ctot: n doubles (zeroed by the caller), sums: 3 doubles (zeroed by the caller) receive
-// [internal weight, total weight 2M, sum of squared community totals].
+// ctot: n doubles (zeroed by the caller), sums: 4 doubles (zeroed by the caller) receive
+// [internal weight, total weight 2M, sum of squared community totals, labels >= n seen].
 cudaError_t launch_modularity(const void *off, bool off64, const uint32_t *tgt, const float *wt, int64_t n,
                               const uint32_t *labels, double *ctot, double *sums, cudaStream_t st) {
   const int g = grid_for(n * 32, 4);

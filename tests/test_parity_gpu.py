@@ -1,0 +1,245 @@
+"""GPU parity through the C ABI (librak_lowmem.so) against the oracle and the reference.
+
+- RAK_MODE_SYNC: bit-identical labels to the reference's CPU per-vertex functions run
+  synchronously, for full runs and for every single iteration from the same snapshot.
+- RAK_MODE_SYNC_SPLIT: bit-identical to the oracle's restatement of the split layout.
+- RAK_MODE_ASYNC (default): valid labellings whose FP64 modularity is within 0.5% of the
+  reference's own GPU νMG8-LPA on the same graph (when its build is present), else of the
+  reference CPU loop.
+- FP64 modularity kernel: relative error <= 1e-9 against the oracle.
+"""
+import numpy as np
+import pytest
+
+import oracle as orc
+import rak_lowmem as rl
+from conftest import golden_graph
+
+pytestmark = pytest.mark.gpu
+
+SMALL_LAYOUT = dict(lane_max=8, hub_min=64, hub_chunk=32)     # forces every region on small graphs
+TINY_LAYOUT = dict(lane_max=2, hub_min=16, hub_chunk=32)
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    c = rl.Context(0)
+    yield c
+    c.close()
+
+
+def graphs():
+    return {
+        "rmat10": rl.gen_rmat(10, 8, seed=1),
+        "rmat11_w": rl.gen_rmat(11, 8, seed=2, w_lo=1.0, w_hi=10.0),
+        "sbm3000": rl.gen_sbm(3000, 30, 12.0, 20.0, seed=3),
+        "lattice": rl.gen_lattice(40, 30, 0.05, 0.02, seed=4),
+    }
+
+
+GRAPHS = graphs()
+
+
+def ocfg(slots, rescan, split=0, layout=None, **kw):
+    lay = (layout["lane_max"], layout["hub_min"], layout["hub_chunk"]) if layout else orc.DEFAULT_LAYOUT
+    return orc.make_opts(slots=slots, rescan=rescan, split=split, layout=lay, **kw)
+
+
+@pytest.mark.parametrize("name", sorted(GRAPHS))
+@pytest.mark.parametrize("slots,rescan", [(8, 1), (8, 0), (4, 1), (16, 0), (2, 1), (1, 0)])
+@pytest.mark.parametrize("layout", [None, SMALL_LAYOUT])
+def test_sync_exact_full_run_matches_oracle(ctx, name, slots, rescan, layout):
+    g = GRAPHS[name]
+    lab, res = ctx.lowmem(g, mode=rl.MODE_SYNC, slots=slots, rescan=rescan, **(layout or {}))
+    ref, it, edges = orc.sync_run(orc.Graph.of(g), ocfg(slots, rescan))
+    assert res.iterations == it
+    np.testing.assert_array_equal(lab, ref)
+    assert res.traversed_edges == edges
+
+
+@pytest.mark.parametrize("name", sorted(GRAPHS))
+def test_sync_exact_every_iteration(ctx, name):
+    """Labels after k iterations equal the oracle's after k iterations, for every k."""
+    g = GRAPHS[name]
+    og = orc.Graph.of(g)
+    o = ocfg(8, 1)
+    vp = np.arange(g.n, dtype=np.uint32)
+    ap = np.ones(g.n, np.uint8)
+    for k in range(1, 8):
+        vp, ap, ch, _, _ = orc.sync_step(og, o, k - 1, vp, ap)
+        lab, res = ctx.lowmem(g, mode=rl.MODE_SYNC, slots=8, max_iterations=k, tolerance=0.0, **SMALL_LAYOUT)
+        np.testing.assert_array_equal(lab, vp, err_msg=f"iteration {k}")
+        assert res.changed_last == ch
+        if ch == 0:
+            break
+
+
+def _golden_names(z):
+    return [str(x) for x in z["graphs"]]
+
+
+@pytest.mark.parametrize("slots,rescan", [(8, 1), (8, 0), (4, 1), (1, 0)])
+@pytest.mark.parametrize("pickless", [0, 1])
+def test_sync_step_matches_reference_golden(ctx, golden, slots, rescan, pickless):
+    """One step from the golden snapshot equals the reference's own synchronous step."""
+    import torch
+    for name in _golden_names(golden):
+        og = golden_graph(golden, name)
+        hg = rl.HostGraph(og.offsets, og.targets, og.weights)
+        rg = rl.ResidentGraph(ctx, hg, **SMALL_LAYOUT)
+        dev = torch.device("cuda:0")
+        vp = torch.from_numpy(golden[f"{name}/snap/labels"].view(np.int32)).to(dev)
+        ap = torch.from_numpy(golden[f"{name}/snap/flags"]).to(dev)
+        vn = torch.empty_like(vp)
+        an = torch.empty_like(ap)
+        ch = rg.step(0, vp, ap, vn, an, mode=rl.MODE_SYNC, slots=slots, rescan=rescan,
+                     pickless_step=1 if pickless else 0, **SMALL_LAYOUT)
+        key = f"{name}/step_{slots}_{rescan}_{pickless}"
+        np.testing.assert_array_equal(vn.cpu().numpy().view(np.uint32), golden[key + "/labels"], err_msg=name)
+        np.testing.assert_array_equal(an.cpu().numpy(), golden[key + "/flags"], err_msg=name)
+        assert ch == int(golden[key + "/changed"]), name
+        rg.close()
+
+
+@pytest.mark.parametrize("name", sorted(GRAPHS))
+@pytest.mark.parametrize("slots", [8, 4, 1, 16])
+@pytest.mark.parametrize("layout", [SMALL_LAYOUT, TINY_LAYOUT, None])
+def test_sync_split_matches_oracle(ctx, name, slots, layout):
+    g = GRAPHS[name]
+    lab, res = ctx.lowmem(g, mode=rl.MODE_SYNC_SPLIT, slots=slots, **(layout or {}))
+    ref, it, edges = orc.sync_run(orc.Graph.of(g), ocfg(slots, 0, split=1, layout=layout))
+    assert res.iterations == it
+    np.testing.assert_array_equal(lab, ref)
+    assert res.traversed_edges == edges
+
+
+@pytest.mark.parametrize("layout", [SMALL_LAYOUT, None])
+def test_sync_split_steps_with_pickless(ctx, layout):
+    import torch
+    g = GRAPHS["rmat11_w"]
+    og = orc.Graph.of(g)
+    rng = np.random.default_rng(7)
+    rg = rl.ResidentGraph(ctx, g, **(layout or {}))
+    for it in range(4):
+        vp = rng.integers(0, g.n // 7, g.n).astype(np.uint32)
+        ap = (rng.random(g.n) < 0.75).astype(np.uint8)
+        tv = torch.from_numpy(vp.view(np.int32)).cuda()
+        ta = torch.from_numpy(ap).cuda()
+        vn, an = torch.empty_like(tv), torch.empty_like(ta)
+        ch = rg.step(it, tv, ta, vn, an, mode=rl.MODE_SYNC_SPLIT, slots=8, pickless_step=2, **(layout or {}))
+        rv, ra, rch, _, _ = orc.sync_step(og, ocfg(8, 0, split=1, layout=layout, pickless_step=2), it, vp, ap)
+        np.testing.assert_array_equal(vn.cpu().numpy().view(np.uint32), rv)
+        np.testing.assert_array_equal(an.cpu().numpy(), ra)
+        assert ch == rch
+    rg.close()
+
+
+def _reference_q(og, slots):
+    if orc.have_ref_cuda():
+        lab, info = orc.ref_lowmem_cuda(og, slots=slots)
+        return orc.modularity(og, lab), "reference GPU"
+    lab, _ = orc.serial_run(og, slots, 0)
+    return orc.modularity(og, lab), "reference CPU loop"
+
+
+@pytest.mark.parametrize("slots", [8, 1])
+def test_async_modularity_close_to_reference(ctx, slots):
+    g = rl.gen_sbm(50000, 100, 16.0, 20.0, seed=11)
+    og = orc.Graph.of(g)
+    lab, res = ctx.lowmem(g, slots=slots, compute_modularity=1)
+    assert lab.max() < g.n
+    q = orc.modularity(og, lab)
+    assert res.modularity == pytest.approx(q, rel=1e-9, abs=1e-12)
+    qref, who = _reference_q(og, slots)
+    assert q >= qref - 0.005 * abs(qref), (q, qref, who)
+    assert 1 <= res.iterations <= 20
+
+
+@pytest.mark.parametrize("name", sorted(GRAPHS))
+def test_async_labels_valid_and_converging(ctx, name):
+    g = GRAPHS[name]
+    lab, res = ctx.lowmem(g, slots=8, **SMALL_LAYOUT)
+    assert lab.dtype == np.uint32 and len(lab) == g.n and lab.max() < g.n
+    # every community name is a vertex id that belongs to a vertex with that label or a neighbour
+    assert res.traversed_edges >= g.m           # the first iteration processes every vertex
+    assert res.iterations >= 1
+
+
+@pytest.mark.parametrize("name", sorted(GRAPHS))
+def test_modularity_kernel_matches_oracle(ctx, name):
+    g = GRAPHS[name]
+    og = orc.Graph.of(g)
+    rng = np.random.default_rng(5)
+    for lab in (np.arange(g.n, dtype=np.uint32), rng.integers(0, 17, g.n).astype(np.uint32),
+                orc.serial_run(og, 8, 1)[0]):
+        q = ctx.modularity(g, lab)
+        assert q == pytest.approx(orc.modularity(og, lab), rel=1e-9, abs=1e-12)
+
+
+def test_edge_cases(ctx):
+    # no vertices
+    empty = rl.HostGraph(np.zeros(1, np.int64), np.zeros(0, np.uint32))
+    lab, res = ctx.lowmem(empty)
+    assert len(lab) == 0
+    # isolated vertices only: nothing moves
+    iso = rl.HostGraph(np.zeros(6, np.int64), np.zeros(0, np.uint32))
+    lab, res = ctx.lowmem(iso, mode=rl.MODE_SYNC)
+    np.testing.assert_array_equal(lab, np.arange(5))
+    assert res.iterations == 1 and res.changed_last == 0
+    # self-loops are skipped; 32- and 64-bit offsets agree; unit weights == explicit ones
+    g = GRAPHS["rmat10"]
+    a, _ = ctx.lowmem(g, mode=rl.MODE_SYNC)
+    b, _ = ctx.lowmem(g.with_offsets32(), mode=rl.MODE_SYNC)
+    ones = rl.HostGraph(g.offsets, g.targets, np.ones(g.m, np.float32))
+    c, _ = ctx.lowmem(ones, mode=rl.MODE_SYNC)
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(a, c)
+    # initial labels and flags are honoured
+    q = (np.arange(g.n) // 4).astype(np.uint32)
+    lab, res = ctx.lowmem(g, q=q, max_iterations=0)
+    np.testing.assert_array_equal(lab, q)
+    lab, res = ctx.lowmem(g, q=q, flags=np.zeros(g.n, np.uint8), mode=rl.MODE_SYNC)
+    np.testing.assert_array_equal(lab, q)
+    assert res.changed_last == 0 and res.traversed_edges == 0
+
+
+def test_errors_are_statuses(ctx):
+    g = GRAPHS["rmat10"]
+    bad = rl.HostGraph(g.offsets, np.where(np.arange(g.m) == 3, g.n + 5, g.targets).astype(np.uint32))
+    with pytest.raises(rl.RakError) as e:
+        ctx.lowmem(bad)
+    assert e.value.status == 2
+    with pytest.raises(rl.RakError) as e:
+        ctx.lowmem(g, slots=3)
+    assert e.value.status == 1
+    with pytest.raises(rl.RakError) as e:
+        ctx.lowmem(g, mode=rl.MODE_ASYNC, rescan=1)
+    assert e.value.status == 7
+    with pytest.raises(rl.RakError) as e:
+        ctx.modularity(g, np.full(g.n, g.n + 1, np.uint32))
+    assert e.value.status == 1
+    lab, _ = ctx.lowmem(g)          # the context is still usable
+    assert lab.max() < g.n
+
+
+def test_device_csr_and_resident_runs(ctx):
+    import torch
+    g = GRAPHS["rmat11_w"]
+    off = torch.from_numpy(g.offsets).cuda()
+    tgt = torch.from_numpy(g.targets.view(np.int32)).cuda()
+    wt = torch.from_numpy(g.weights).cuda()
+    csr = rl.device_csr(off, tgt, wt)
+    out = torch.empty(g.n, dtype=torch.int32, device="cuda")
+    res = ctx.lowmem_device(csr, out, mode=rl.MODE_SYNC)
+    host, hres = ctx.lowmem(g, mode=rl.MODE_SYNC)
+    np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), host)
+    assert res.iterations == hres.iterations
+    rg = rl.ResidentGraph(ctx, csr)
+    out2 = torch.empty_like(out)
+    r2 = rg.run(out2, mode=rl.MODE_SYNC, repeat=3)
+    np.testing.assert_array_equal(out2.cpu().numpy().view(np.uint32), host)
+    assert r2.time_ms > 0 and rg.device_bytes() > 0
+    assert ctx.modularity(csr, out2) == pytest.approx(orc.modularity(orc.Graph.of(g), host), rel=1e-9)
+    rg.close()
