@@ -1,0 +1,375 @@
+#!/usr/bin/env python3
+"""Headline benchmark: νMG8-LPA (8-slot weighted Misra-Gries label propagation) on one graph.
+
+Metric: traversed edges per second (sum over iterations of the degrees of the vertices each
+iteration processes), with the achieved HBM bandwidth of the LPA kernel against the measured B200
+copy peak. A step is one complete run -- labels and flags initialised, then iterations until
+convergence (tolerance 0.05, at most 20) -- on a graph already resident in HBM.
+
+Default workload: symmetric R-MAT scale 24, edge factor 32, (a,b,c,d) = (0.57,0.19,0.19,0.05),
+float32 weights uniform in [1,10) (same value both directions), int32 CSR: the degree-regime
+coverage graph the reference's νMG8/νBM comparison is quoted on. Synthetic and seeded (seed 42)
+because the reference's SuiteSparse inputs are not available.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+With --gpus N > 1 (launched by torch.distributed.run) every rank runs an independent replica of
+the workload on its own GPU (the path does not shard a single graph): weak scaling, no collective
+on the data path; timing is the max over ranks.
+
+--impl reference times the reference's own CPU implementation, rakLowmemStaticOmp<true,true,8>
+compiled from its sources into oracle/_ref, on the host cores: each step is its first iteration
+over the whole graph (every vertex affected), a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "rak-lowmem-communities-cuda_b200")
+sys.path.insert(0, PKG)
+
+WORKLOADS = {
+    # configs: R-MAT scale 24 / ef 32 / U[1,10) weights / int32 CSR (degree-regime graph 1)
+    "rmat24_ef32_w": dict(kind="rmat", scale=24, ef=32, w=(1.0, 10.0), off_bits=32),
+    # a smaller graph of the same family (0.5 GB, larger than L2) for profiling captures
+    "rmat20_ef32_w": dict(kind="rmat", scale=20, ef=32, w=(1.0, 10.0), off_bits=32),
+    # scale-16 graph of the reference's CPU-runnable case (unit weights)
+    "rmat16_ef16": dict(kind="rmat", scale=16, ef=16, w=(1.0, 1.0), off_bits=32),
+    # largest single graph: scale 27 / ef 16 / unit weights / int64 offsets
+    "rmat27_ef16": dict(kind="rmat", scale=27, ef=16, w=(1.0, 1.0), off_bits=64),
+    # road-like lattice with 2^25 vertices (degree-regime graph 2)
+    "lattice25": dict(kind="lattice", width=8192, height=4096, p_delete=0.05, shortcut=0.01, off_bits=32),
+}
+DEFAULT_WORKLOAD = "rmat24_ef32_w"
+METRIC = "traversed edges/sec (νMG8-LPA, whole run to convergence)"
+UNIT = "edges/s"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_graph(spec, threads=0):
+    import rak_lowmem as rl
+    if spec["kind"] == "rmat":
+        g = rl.gen_rmat(spec["scale"], spec["ef"], 0.57, 0.19, 0.19, 42, spec["w"][0], spec["w"][1], threads)
+    else:
+        g = rl.gen_lattice(spec["width"], spec["height"], spec["p_delete"], spec["shortcut"], 42, threads)
+    return g
+
+
+def describe(name, spec, g):
+    d = {"workload": name, "n": int(g.n), "m": int(g.m), "offsets": f"int{spec['off_bits']}",
+         "targets": "uint32", "weights": "float32 U[1,10)" if g.weights is not None else "unit (no weight array)",
+         "seed": 42, "tolerance": 0.05, "max_iterations": 20}
+    if spec["kind"] == "rmat":
+        d.update(generator=f"symmetric R-MAT scale {spec['scale']} ef {spec['ef']} (0.57,0.19,0.19,0.05), "
+                           "self-loops and duplicates removed, ids not permuted")
+    else:
+        d.update(generator=f"{spec['width']}x{spec['height']} 4-neighbour lattice, {spec['p_delete']:.0%} edges "
+                           f"deleted, {spec['shortcut']:.0%} shortcuts")
+    return d
+
+
+def graph_bytes(g, off_bits):
+    return (g.n + 1) * off_bits // 8 + g.m * 4 + (g.m * 4 if g.weights is not None else 0)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(self.gpu_id)], stdout=subprocess.PIPE,
+                                      stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.p:
+            time.sleep(0.25)
+            self.p.terminate()
+            try:
+                out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                out, _ = self.p.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_for(workload):
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        d = json.load(open(p)).get(workload)
+        if d:
+            return d
+    return None
+
+
+def algorithmic_bytes(res, off_bytes, weighted):
+    """Bytes the LPA kernel must move (per run): for each processed vertex 12*deg (target, weight,
+    neighbour label; 8*deg without weights) + offset pair + own label + flag read/write; for each
+    moved vertex its label write plus 5*deg to re-read targets and mark neighbour flags."""
+    per_edge = 12 if weighted else 8
+    return (per_edge * res.traversed_edges + (off_bytes + 4 + 1 + 1) * res.processed_vertices
+            + 4 * res.moved_vertices + 5 * res.moved_edges)
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args, spec, world, rank):
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    threads = os.cpu_count() or 1
+    g = make_graph(spec, threads)
+    og = orc.Graph.of(g)
+    log(f"[reference] graph n={g.n} m={g.m}; rakLowmemStaticOmp<MG8,rescan> first iteration, {threads} threads")
+    times = []
+    for i in range(args.warmup + args.steps):
+        _, it, tms = orc.ref_lowmem_omp(og, 8, 1, tolerance=0.05, max_iterations=1, threads=threads)
+        if i >= args.warmup:
+            times.append(tms / 1e3)
+    value = g.m * len(times) / sum(times)
+    sample = (f"first iteration (all {g.n} vertices affected, {g.m} edges) of the reference "
+              f"rakLowmemStaticOmp<MULTI=1,RESCAN=1,SLOTS=8> per step")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": describe(args.workload, spec, g),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(g, budget_s=20.0):
+    """The reference CPU MG8-LPA (oracle/_ref) on the host cores: first iteration over the graph,
+    repeated while within the budget. Returns the cpu_baseline object."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    if not orc.have_ref_cpu():
+        return None
+    threads = os.cpu_count() or 1
+    og = orc.Graph.of(g)
+    times = []
+    t0 = time.time()
+    while not times or (time.time() - t0 < budget_s and len(times) < 3):
+        _, _, tms = orc.ref_lowmem_omp(og, 8, 1, tolerance=0.05, max_iterations=1, threads=threads)
+        times.append(tms / 1e3)
+    return {"value": g.m / min(times), "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"first iteration (all vertices affected, {g.m} edges) of rakLowmemStaticOmp<1,1,8> "
+                      f"on the same graph, best of {len(times)}"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    spec = WORKLOADS[args.workload]
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, spec, world, rank)
+        return
+
+    import torch
+    import rak_lowmem as rl
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+
+    def barrier():
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    threads = max(1, (os.cpu_count() or 1) // world)
+    t0 = time.time()
+    g = make_graph(spec, threads)
+    if spec["off_bits"] == 32:
+        g = g.with_offsets32()
+    log(f"[rank {rank}] graph n={g.n} m={g.m} generated in {time.time() - t0:.1f}s")
+    ctx = rl.Context(local)
+    # A dedicated stream: the library's work and the timing events share it.
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    rg = rl.ResidentGraph(ctx, g)
+    membership = torch.empty(g.n, dtype=torch.int32, device="cuda")
+    opts = dict(slots=args.slots)
+
+    for _ in range(args.warmup):
+        rg.run(membership, **opts)
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    results = []
+    gpu_id = torch.cuda.get_device_properties(local).uuid
+    gpu_id = f"GPU-{gpu_id}" if gpu_id else local
+    with ClockSampler(gpu_id) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            results.append(rg.run(membership, **opts))
+        ev1.record(stream)
+        barrier()
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    edges = sum(r.traversed_edges for r in results)
+    t_max = elapsed
+    total_edges = edges
+    if pg:
+        t = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        t_max = float(t.item())
+        e = torch.tensor([edges], dtype=torch.float64, device="cuda")
+        pg.all_reduce(e, op=pg.ReduceOp.SUM)
+        total_edges = float(e.item())
+    value = total_edges / t_max
+
+    # roofline of the persistent LPA kernel, from the runs just timed
+    off_bytes = spec["off_bits"] // 8
+    weighted = g.weights is not None
+    loop_s = sum(r.loop_ms for r in results) / 1e3 / len(results)
+    bytes_per_launch = sum(algorithmic_bytes(r, off_bytes, weighted) for r in results) / len(results)
+    achieved = bytes_per_launch / loop_s / 1e9
+    peak, peak_kind = peaks()
+    traffic = traffic_for(args.workload)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": f"{peak_kind} HBM copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
+                "kernel": "rak::lpa_run (persistent, all iterations in one launch)",
+                "algorithmic_bytes_per_launch": bytes_per_launch, "launch_ms": loop_s * 1e3,
+                "traffic": traffic["bytes_per_launch"] if traffic else None}
+    if traffic:
+        roofline["traffic_source"] = traffic.get("source")
+
+    # quality (outside the timed region)
+    res_q = rg.run(membership, compute_modularity=1, **opts)
+
+    # end to end through the C ABI with host buffers in pinned memory
+    # the host CSR arrays are page-locked in place (no second copy)
+    cudart = torch.cuda.cudart()
+    host_arrays = [g.offsets, g.targets] + ([g.weights] if weighted else [])
+    for arr in host_arrays:
+        assert int(cudart.cudaHostRegister(arr.ctypes.data, arr.nbytes, 0)) == 0, "cudaHostRegister failed"
+    hg = g
+    out_host = torch.empty(g.n, dtype=torch.int32).pin_memory()
+    e2e_edges, e2e_time = 0, 0.0
+    rg.close()
+    for i in range(args.e2e_steps + 1):
+        barrier()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        c = hg.csr()
+        o = rl.options(**opts)
+        r = rl.rak_result()
+        s0.record(stream)
+        st = rl._lib.rak_lowmem_cuda(ctx.handle, rl.C.byref(c), None, rl.C.byref(o), out_host.data_ptr(),
+                                     rl.C.byref(r))
+        s1.record(stream)
+        torch.cuda.synchronize()
+        if st != 0:
+            raise rl.RakError(st, ctx.last_error())
+        if i > 0:   # the first call warms the allocator
+            e2e_time += s0.elapsed_time(s1) / 1e3
+            e2e_edges += r.traversed_edges
+    for arr in host_arrays:
+        cudart.cudaHostUnregister(arr.ctypes.data)
+    e2e_t = torch.tensor([e2e_time], dtype=torch.float64, device="cuda")
+    e2e_e = torch.tensor([float(e2e_edges)], dtype=torch.float64, device="cuda")
+    if pg:
+        pg.all_reduce(e2e_t, op=pg.ReduceOp.MAX)
+        pg.all_reduce(e2e_e, op=pg.ReduceOp.SUM)
+    e2e = {"value": float(e2e_e.item()) / float(e2e_t.item()), "unit": UNIT,
+           "h2d_bytes_per_step": graph_bytes(g, spec["off_bits"]), "d2h_bytes_per_step": g.n * 4,
+           "path": "rak_lowmem_cuda (C ABI) with pinned host CSR: upload, plan, run, membership read-back",
+           "steps": args.e2e_steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(g)
+
+    if rank == 0:
+        last = results[-1]
+        cfg = describe(args.workload, spec, g)
+        cfg.update(slots=args.slots, mode="async (in-place, pickless every 8th iteration)",
+                   parallelism=f"replicas x{world}" if world > 1 else "single GPU",
+                   l2=f"inputs larger than L2: graph {graph_bytes(g, spec['off_bits']) / 1e9:.1f} GB vs 126 MB L2")
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+                "gpu_launches": 3 * args.steps,
+                "run": {"iterations": last.iterations, "traversed_edges_per_step": last.traversed_edges,
+                        "processed_vertices_per_step": last.processed_vertices,
+                        "moved_vertices_per_step": last.moved_vertices, "loop_ms": last.loop_ms,
+                        "time_ms": last.time_ms, "modularity": res_q.modularity,
+                        "memory_gb": last.memory_gb, "plan_ms": last.plan_ms,
+                        "peak_device_bytes": res_q.peak_device_bytes}}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

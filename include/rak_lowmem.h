@@ -108,6 +108,10 @@ typedef struct rak_result {
   uint64_t traversed_edges;    /* sum over iterations of the degrees of the vertices processed */
   uint64_t processed_vertices; /* sum over iterations of the vertices processed */
   uint64_t changed_last;       /* vertices that changed label in the last iteration */
+  uint64_t moved_vertices;     /* sum over iterations of the vertices that changed label */
+  uint64_t moved_edges;        /* sum over iterations of the degrees of the vertices that moved */
+  float loop_ms;               /* device time of the iterations alone (the persistent kernel) */
+  float reserved_f;
   double modularity;           /* when requested, else NaN */
 } rak_result;
 

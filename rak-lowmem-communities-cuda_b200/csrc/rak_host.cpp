@@ -362,7 +362,7 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
   RAK_TRY(ctx, b.moved.alloc(nh * 4, tr));
   RAK_TRY(ctx, b.skk.alloc(nc * size_t(r.slots) * 4, tr));
   RAK_TRY(ctx, b.skw.alloc(nc * size_t(r.slots) * 4, tr));
-  RAK_TRY(ctx, b.stats.alloc(size_t(iters) * 4 * 8, tr));
+  RAK_TRY(ctx, b.stats.alloc(size_t(iters) * rak::STATS_STRIDE * 8, tr));
   RAK_TRY(ctx, b.rs.alloc(sizeof(rak::RunStateHost), tr));
 
   rak::LpaArgs a{};
@@ -377,9 +377,9 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
   a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.timeout_ns = 20LL * 1000 * 1000 * 1000;
 
   Events ev;
-  float t_init = 0, t_mark = 0, t_all = 0;
+  float t_init = 0, t_mark = 0, t_all = 0, t_loop = 0;
   rak::RunStateHost hs{};
-  std::vector<unsigned long long> stats(size_t(iters) * 4, 0);
+  std::vector<unsigned long long> stats(size_t(iters) * rak::STATS_STRIDE, 0);
   for (int rep = 0; rep < r.repeat; ++rep) {
     RAK_TRY(ctx, cudaMemsetAsync(b.arrive.p, 0, b.arrive.bytes, st));
     RAK_TRY(ctx, cudaMemsetAsync(b.claim.p, 0, b.claim.bytes, st));
@@ -399,6 +399,7 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
     RAK_TRY(ctx, cudaStreamSynchronize(st));
     t_init += ev.ms(0, 1);
     t_mark += ev.ms(1, 2);
+    t_loop += ev.ms(2, 3);
     t_all += ev.ms(0, 3);
   }
   RAK_TRY(ctx, cudaMemcpyAsync(&hs, b.rs.p, sizeof(hs), cudaMemcpyDeviceToHost, st));
@@ -416,9 +417,16 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
     res->time_ms = t_all / float(r.repeat);
     res->initialization_time_ms = t_init / float(r.repeat);
     res->marking_time_ms = t_mark / float(r.repeat);
-    res->traversed_edges = res->processed_vertices = 0;
-    for (int i = 0; i < done; ++i) { res->traversed_edges += stats[i * 4 + 1]; res->processed_vertices += stats[i * 4 + 2]; }
-    res->changed_last = done > 0 ? stats[(done - 1) * 4] : 0;
+    res->loop_ms = t_loop / float(r.repeat);
+    res->traversed_edges = res->processed_vertices = res->moved_vertices = res->moved_edges = 0;
+    for (int i = 0; i < done; ++i) {
+      const unsigned long long *st_i = &stats[size_t(i) * rak::STATS_STRIDE];
+      res->traversed_edges += st_i[rak::STAT_EDGES];
+      res->processed_vertices += st_i[rak::STAT_PROCESSED];
+      res->moved_vertices += st_i[rak::STAT_CHANGED];
+      res->moved_edges += st_i[rak::STAT_MOVED_EDGES];
+    }
+    res->changed_last = done > 0 ? stats[size_t(done - 1) * rak::STATS_STRIDE + rak::STAT_CHANGED] : 0;
     res->memory_gb = float(double(b.bytes() + size_t(n) * 4 + gr->plan_bytes) / (1024.0 * 1024.0 * 1024.0));
     res->plan_ms = gr->plan_ms;
   }
@@ -623,7 +631,7 @@ rak_status rak_graph_step(rak_ctx *ctx, rak_graph *gr, const rak_options *o, int
   RAK_TRY(ctx, b.moved.alloc(nh * 4, nullptr));
   RAK_TRY(ctx, b.skk.alloc(nc * size_t(r.slots) * 4, nullptr));
   RAK_TRY(ctx, b.skw.alloc(nc * size_t(r.slots) * 4, nullptr));
-  RAK_TRY(ctx, b.stats.alloc(4 * 8, nullptr));
+  RAK_TRY(ctx, b.stats.alloc(rak::STATS_STRIDE * 8, nullptr));
   RAK_TRY(ctx, b.rs.alloc(sizeof(rak::RunStateHost), nullptr));
   RAK_TRY(ctx, cudaMemsetAsync(b.arrive.p, 0, b.arrive.bytes, st));
   RAK_TRY(ctx, cudaMemsetAsync(b.claim.p, 0, b.claim.bytes, st));
@@ -650,7 +658,7 @@ rak_status rak_graph_step(rak_ctx *ctx, rak_graph *gr, const rak_options *o, int
   a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.timeout_ns = 20LL * 1000 * 1000 * 1000;
   int grid = 0;
   RAK_TRY(ctx, rak::launch_lpa(a, r.slots, r.mode, gr->off64, st, &grid));
-  unsigned long long s[4] = {0, 0, 0, 0};
+  unsigned long long s[rak::STATS_STRIDE] = {};
   rak::RunStateHost hs{};
   RAK_TRY(ctx, cudaMemcpyAsync(s, b.stats.p, sizeof(s), cudaMemcpyDeviceToHost, st));
   RAK_TRY(ctx, cudaMemcpyAsync(&hs, b.rs.p, sizeof(hs), cudaMemcpyDeviceToHost, st));

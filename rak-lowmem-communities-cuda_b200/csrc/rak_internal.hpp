@@ -74,7 +74,7 @@ struct LpaArgs {
   int32_t *hub_moved;          // per split vertex: last iteration it moved in (-1: never)
   uint32_t *sk_keys;           // per chunk: slots keys of its partial sketch
   float *sk_wts;               // per chunk: slots weights
-  unsigned long long *stats;   // per iteration: changed, edges, processed, split vertices moved
+  unsigned long long *stats;   // per iteration, STATS_STRIDE slots (STAT_* below)
   void *rs;                    // RunState
   int iters;
   int start_iter;
@@ -86,6 +86,10 @@ struct LpaArgs {
 };
 
 enum Mode { MODE_ASYNC = 0, MODE_SYNC = 1, MODE_SPLIT = 2 };
+
+// Per-iteration counters written by the LPA kernel.
+enum Stat { STAT_CHANGED = 0, STAT_EDGES = 1, STAT_PROCESSED = 2, STAT_HUBS_MOVED = 3, STAT_MOVED_EDGES = 4 };
+constexpr int STATS_STRIDE = 8;
 
 // Persistent cooperative launch of all iterations; grid chosen from occupancy.
 cudaError_t launch_lpa(const LpaArgs &a, int slots, int mode, bool off64, cudaStream_t st, int *grid_out);

@@ -20,6 +20,7 @@ namespace rak {
 
 struct Counters {
   unsigned long long edges;
+  unsigned long long moved_edges;
   unsigned int changed;
   unsigned int processed;
 };
@@ -177,6 +178,7 @@ __device__ __forceinline__ void lane_item(const LpaArgs &a, const Regions &rg, c
   }
   if (moved) {
     cnt.changed += 1;
+    cnt.moved_edges += (unsigned long long)(ee - eb);
     mark_range(u, eb, ee, 1, g.tgt, fout);
   }
 }
@@ -220,7 +222,7 @@ __device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, 
     } else {
       vout[u] = moved ? c : d;
     }
-    if (moved) cnt.changed += 1;
+    if (moved) { cnt.changed += 1; cnt.moved_edges += (unsigned long long)(ee - eb); }
   }
   if (moved) mark_range(u, eb + s, ee, G, g.tgt, fout);
 }
@@ -253,7 +255,7 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
     if (lane == 0) {
       vout[u] = moved ? c : d;
       if (active) { cnt.processed += 1; cnt.edges += (unsigned long long)(ee - eb); }
-      if (moved) cnt.changed += 1;
+      if (moved) { cnt.changed += 1; cnt.moved_edges += (unsigned long long)(ee - eb); }
     }
     if (moved) mark_range(u, eb + lane, ee, 32, g.tgt, fout);
     return;
@@ -335,8 +337,9 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
       }
       if (moved) {
         cnt.changed += 1;
+        cnt.moved_edges += (unsigned long long)(ee - eb);
         a.hub_moved[h] = it;
-        atomicAdd(a.stats + 4 * it + 3, 1ull);
+        atomicAdd(a.stats + STATS_STRIDE * it + STAT_HUBS_MOVED, 1ull);
       }
     }
   }
@@ -349,12 +352,12 @@ __global__ void __launch_bounds__(256, 2) lpa_run(const LpaArgs a) {
   const int lane = threadIdx.x & 31;
   const int64_t gw = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
-  __shared__ unsigned long long blk[3];
+  __shared__ unsigned long long blk[4];
   __shared__ Regions rg;  // copied once: indexed by region at run time
   if (threadIdx.x == 0) rg = a.rg;
   unsigned int epoch = 0;
   for (int it = 0; it < a.iters; ++it) {
-    if (threadIdx.x < 3) blk[threadIdx.x] = 0;
+    if (threadIdx.x < 4) blk[threadIdx.x] = 0;
     __syncthreads();
     const int l = a.start_iter + it;
     const bool pickless = a.pickless_step > 0 && l % a.pickless_step == 0;
@@ -363,7 +366,7 @@ __global__ void __launch_bounds__(256, 2) lpa_run(const LpaArgs a) {
     uint32_t *vout = MODE == MODE_ASYNC ? a.vcom0 : (odd ? a.vcom0 : a.vcom1);
     uint8_t *fin = odd ? a.aff1 : a.aff0;
     uint8_t *fout = MODE == MODE_ASYNC ? a.aff0 : (odd ? a.aff0 : a.aff1);
-    Counters cnt{0, 0, 0};
+    Counters cnt{0, 0, 0, 0};
     const int64_t total = rg.ibegin[NREG];
     for (int64_t item = gw; item < total; item += nw) {
       int r = 0;
@@ -376,20 +379,25 @@ __global__ void __launch_bounds__(256, 2) lpa_run(const LpaArgs a) {
     const unsigned long long ch = warp_sum((unsigned long long)cnt.changed);
     const unsigned long long ed = warp_sum(cnt.edges);
     const unsigned long long pr = warp_sum((unsigned long long)cnt.processed);
+    const unsigned long long me = warp_sum(cnt.moved_edges);
     if (lane == 0) {
       if (ch) atomicAdd(&blk[0], ch);
       if (ed) atomicAdd(&blk[1], ed);
       if (pr) atomicAdd(&blk[2], pr);
+      if (me) atomicAdd(&blk[3], me);
     }
     __syncthreads();
-    if (threadIdx.x < 3 && blk[threadIdx.x]) atomicAdd(a.stats + 4 * it + threadIdx.x, blk[threadIdx.x]);
+    if (threadIdx.x < 4 && blk[threadIdx.x]) {
+      const int slot = threadIdx.x == 3 ? STAT_MOVED_EDGES : int(threadIdx.x);
+      atomicAdd(a.stats + STATS_STRIDE * it + slot, blk[threadIdx.x]);
+    }
     if (!grid_barrier(rs, ++epoch, a.timeout_ns)) return;
-    const unsigned long long changed = __ldcg(a.stats + 4 * it);
+    const unsigned long long changed = __ldcg(a.stats + STATS_STRIDE * it + STAT_CHANGED);
     const bool test = !pickless || a.check_on_pickless;
     const bool done = it + 1 >= a.iters || (test && double(changed) / double(a.n) <= a.tolerance);
     // The synchronous split mode completes the next flags even on the last iteration, so a
     // single step returns them whole.
-    if (MODE != MODE_SYNC && (!done || MODE == MODE_SPLIT) && a.nchunks > 0 && __ldcg(a.stats + 4 * it + 3) > 0) {
+    if (MODE != MODE_SYNC && (!done || MODE == MODE_SPLIT) && a.nchunks > 0 && __ldcg(a.stats + STATS_STRIDE * it + STAT_HUBS_MOVED) > 0) {
       // Second phase: neighbours of split vertices that moved this iteration.
       for (int64_t i = gw; i < a.nchunks; i += nw) {
         const uint32_t h = __ldg(a.chunk_hub + i);

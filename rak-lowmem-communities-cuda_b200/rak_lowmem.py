@@ -51,7 +51,8 @@ class rak_result(C.Structure):
                 ("initialization_time_ms", C.c_float), ("memory_gb", C.c_float), ("plan_ms", C.c_float),
                 ("h2d_ms", C.c_float), ("d2h_ms", C.c_float), ("peak_device_bytes", C.c_uint64),
                 ("traversed_edges", C.c_uint64), ("processed_vertices", C.c_uint64),
-                ("changed_last", C.c_uint64), ("modularity", C.c_double)]
+                ("changed_last", C.c_uint64), ("moved_vertices", C.c_uint64), ("moved_edges", C.c_uint64),
+                ("loop_ms", C.c_float), ("reserved_f", C.c_float), ("modularity", C.c_double)]
 
 
 class rak_host_csr(C.Structure):
@@ -129,6 +130,10 @@ class Result:
     traversed_edges: int
     processed_vertices: int
     changed_last: int
+    moved_vertices: int
+    moved_edges: int
+    loop_ms: float
+    reserved_f: float
     modularity: float
 
     @staticmethod
