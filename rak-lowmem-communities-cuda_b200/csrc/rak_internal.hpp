@@ -88,7 +88,7 @@ struct LpaArgs {
 enum Mode { MODE_ASYNC = 0, MODE_SYNC = 1, MODE_SPLIT = 2 };
 
 // Per-iteration counters written by the LPA kernel.
-enum Stat { STAT_CHANGED = 0, STAT_EDGES = 1, STAT_PROCESSED = 2, STAT_HUBS_MOVED = 3, STAT_MOVED_EDGES = 4 };
+enum Stat { STAT_CHANGED = 0, STAT_EDGES = 1, STAT_PROCESSED = 2, STAT_HUBS_MOVED = 3, STAT_MOVED_EDGES = 4, STAT_WORK = 5 };
 constexpr int STATS_STRIDE = 8;
 
 // Persistent cooperative launch of all iterations; grid chosen from occupancy.

@@ -9,9 +9,9 @@
 // count and the convergence test stay on the device; iterations are separated by a bounded grid
 // barrier instead of kernel launches and host round trips.
 //
-// Work is a static list of items over the plan's regions (rak_internal.hpp): warp w takes items
-// w, w + W, w + 2W, ... of every iteration, so each warp gets a similar mix of heavy and light
-// items. Sketches live in registers, one per lane.
+// Work is a list of items over the plan's regions (rak_internal.hpp), heaviest first; warps take
+// the next item from a per-iteration counter, so the load balances dynamically. Sketches live in
+// registers, one per lane.
 #pragma once
 #include "rak_device.cuh"
 #include "rak_internal.hpp"
@@ -38,27 +38,42 @@ __device__ __forceinline__ float edge_w(const float *wt, int64_t e) {
   else return __ldg(wt + e);
 }
 
-// Sequential sketch of edges e, e+st, ... < ee of u (self-loops skipped), four edges in flight.
-// Labels are read with plain loads: they change during the launch.
+// Sequential sketch of edges e, e+st, ... < ee of u (self-loops skipped), in edge order.
+// Software-pipelined in batches of four: the next batch's targets and weights are loaded while
+// the current batch's labels are gathered and accumulated. Positions past the end are given the
+// target u itself, which the self-loop rule skips. Labels are read with plain loads: they change
+// during the launch.
 template <int S, bool UNIT>
 __device__ __forceinline__ void scan_range(Sketch<S> &sk, uint32_t u, int64_t e, int64_t ee, int st,
                                            const uint32_t *tgt, const float *wt, const uint32_t *vin) {
-  for (; e + 3 * int64_t(st) < ee; e += 4 * int64_t(st)) {
-    const uint32_t v0 = __ldg(tgt + e), v1 = __ldg(tgt + e + st), v2 = __ldg(tgt + e + 2 * st),
-                   v3 = __ldg(tgt + e + 3 * st);
-    const float w0 = edge_w<UNIT>(wt, e), w1 = edge_w<UNIT>(wt, e + st), w2 = edge_w<UNIT>(wt, e + 2 * st),
-                w3 = edge_w<UNIT>(wt, e + 3 * st);
-    const uint32_t c0 = vin[v0], c1 = vin[v1], c2 = vin[v2], c3 = vin[v3];
-    if (v0 != u) sk_acc(sk, c0, w0);
-    if (v1 != u) sk_acc(sk, c1, w1);
-    if (v2 != u) sk_acc(sk, c2, w2);
-    if (v3 != u) sk_acc(sk, c3, w3);
+  constexpr int B = 4;
+  uint32_t t[B];
+  float w[B];
+#pragma unroll
+  for (int j = 0; j < B; ++j) {
+    const int64_t x = e + int64_t(j) * st;
+    t[j] = x < ee ? __ldg(tgt + x) : u;
+    w[j] = x < ee ? edge_w<UNIT>(wt, x) : 0.0f;
   }
-  for (; e < ee; e += st) {
-    const uint32_t v = __ldg(tgt + e);
-    const float w = edge_w<UNIT>(wt, e);
-    const uint32_t c = vin[v];
-    if (v != u) sk_acc(sk, c, w);
+  while (e < ee) {
+    uint32_t c[B];
+#pragma unroll
+    for (int j = 0; j < B; ++j) c[j] = vin[t[j]];
+    const int64_t en = e + int64_t(B) * st;
+    uint32_t t2[B];
+    float w2[B];
+#pragma unroll
+    for (int j = 0; j < B; ++j) {
+      const int64_t x = en + int64_t(j) * st;
+      t2[j] = x < ee ? __ldg(tgt + x) : u;
+      w2[j] = x < ee ? edge_w<UNIT>(wt, x) : 0.0f;
+    }
+#pragma unroll
+    for (int j = 0; j < B; ++j)
+      if (t[j] != u) sk_acc(sk, c[j], w[j]);
+#pragma unroll
+    for (int j = 0; j < B; ++j) { t[j] = t2[j]; w[j] = w2[j]; }
+    e = en;
   }
 }
 
@@ -144,20 +159,36 @@ __device__ __forceinline__ bool move_rule(float w, uint32_t c, uint32_t d, bool 
   return w > 0.0f && c != d && !(pickless && c > d);
 }
 
-// Region 6: one lane per vertex.
+// Region 6: one lane per vertex. Items are collected into a per-warp queue of active vertices
+// (inactive ones are settled at once), and the queue is processed 32 vertices at a time so every
+// lane has work; region 6 is sorted by degree, so a batch holds vertices of similar degree.
 template <int S, int MODE, class O, bool UNIT>
-__device__ __forceinline__ void lane_item(const LpaArgs &a, const Regions &rg, const G_<O> &g, int64_t local, bool pickless,
-                                          const uint32_t *vin, uint32_t *vout, uint8_t *fin, uint8_t *fout,
-                                          Counters &cnt) {
+__device__ __forceinline__ int lane_collect(const LpaArgs &a, const Regions &rg, int64_t local, const uint32_t *vin,
+                                            uint32_t *vout, const uint8_t *fin, uint32_t *q, int qn) {
   const int lane = threadIdx.x & 31;
   const int64_t idx = local * 32 + lane;
-  if (idx >= rg.vcount[REG_LANE]) return;
-  const uint32_t u = __ldg(a.order + rg.vbegin[REG_LANE] + idx);
-  const uint32_t d = vin[u];
-  if (!fin[u]) {
-    if constexpr (MODE != MODE_ASYNC) vout[u] = d;
-    return;
+  bool act = false;
+  uint32_t u = 0;
+  if (idx < rg.vcount[REG_LANE]) {
+    u = __ldg(a.order + rg.vbegin[REG_LANE] + idx);
+    act = fin[u] != 0;
+    if constexpr (MODE != MODE_ASYNC)
+      if (!act) vout[u] = vin[u];
   }
+  const unsigned m = __ballot_sync(FULL, act);
+  if (act) q[qn + __popc(m & ((1u << lane) - 1u))] = u;
+  __syncwarp();
+  return qn + __popc(m);
+}
+
+template <int S, int MODE, class O, bool UNIT>
+__device__ __forceinline__ void lane_batch(const LpaArgs &a, const G_<O> &g, const uint32_t *q, int count,
+                                           bool pickless, const uint32_t *vin, uint32_t *vout, uint8_t *fin,
+                                           uint8_t *fout, Counters &cnt) {
+  const int lane = threadIdx.x & 31;
+  if (lane >= count) return;
+  const uint32_t u = q[lane];
+  const uint32_t d = vin[u];
   const int64_t eb = int64_t(__ldg(g.off + u)), ee = int64_t(__ldg(g.off + u + 1));
   Sketch<S> sk;
   sk_clear(sk);
@@ -346,7 +377,7 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
 }
 
 template <int S, int MODE, class O, bool UNIT>
-__global__ void __launch_bounds__(256, 2) lpa_run(const LpaArgs a) {
+__global__ void __launch_bounds__(256, 3) lpa_run(const LpaArgs a) {
   const G_<O> g{static_cast<const O *>(a.off), a.tgt, a.wt};
   RunState *rs = static_cast<RunState *>(a.rs);
   const int lane = threadIdx.x & 31;
@@ -354,6 +385,7 @@ __global__ void __launch_bounds__(256, 2) lpa_run(const LpaArgs a) {
   const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
   __shared__ unsigned long long blk[4];
   __shared__ Regions rg;  // copied once: indexed by region at run time
+  __shared__ uint32_t lq[8][64];  // per-warp queue of active one-lane vertices
   if (threadIdx.x == 0) rg = a.rg;
   unsigned int epoch = 0;
   for (int it = 0; it < a.iters; ++it) {
@@ -368,14 +400,34 @@ __global__ void __launch_bounds__(256, 2) lpa_run(const LpaArgs a) {
     uint8_t *fout = MODE == MODE_ASYNC ? a.aff0 : (odd ? a.aff0 : a.aff1);
     Counters cnt{0, 0, 0, 0};
     const int64_t total = rg.ibegin[NREG];
-    for (int64_t item = gw; item < total; item += nw) {
+    unsigned long long *work = a.stats + STATS_STRIDE * it + STAT_WORK;
+    uint32_t *q = lq[threadIdx.x >> 5];
+    int qn = 0;
+    for (;;) {
+      unsigned long long got = 0;
+      if (lane == 0) got = atomicAdd(work, 1ull);
+      const int64_t item = int64_t(__shfl_sync(FULL, got, 0));
+      if (item >= total) break;
       int r = 0;
       while (item >= rg.ibegin[r + 1]) ++r;
       const int64_t local = item - rg.ibegin[r];
-      if (r == REG_HUB) hub_item<S, MODE, O, UNIT>(a, rg, g, local, it, pickless, vin, vout, fin, fout, cnt);
-      else if (r == REG_LANE) lane_item<S, MODE, O, UNIT>(a, rg, g, local, pickless, vin, vout, fin, fout, cnt);
-      else group_item<S, MODE, O, UNIT>(a, rg, g, r, local, pickless, vin, vout, fin, fout, cnt);
+      if (r == REG_LANE) {
+        qn = lane_collect<S, MODE, O, UNIT>(a, rg, local, vin, vout, fin, q, qn);
+        if (qn >= 32) {
+          lane_batch<S, MODE, O, UNIT>(a, g, q, 32, pickless, vin, vout, fin, fout, cnt);
+          __syncwarp();
+          if (lane < qn - 32) q[lane] = q[32 + lane];
+          __syncwarp();
+          qn -= 32;
+        }
+      } else if (r == REG_HUB) {
+        hub_item<S, MODE, O, UNIT>(a, rg, g, local, it, pickless, vin, vout, fin, fout, cnt);
+      } else {
+        group_item<S, MODE, O, UNIT>(a, rg, g, r, local, pickless, vin, vout, fin, fout, cnt);
+      }
     }
+    if (qn > 0) lane_batch<S, MODE, O, UNIT>(a, g, q, qn, pickless, vin, vout, fin, fout, cnt);
+    __syncwarp();
     const unsigned long long ch = warp_sum((unsigned long long)cnt.changed);
     const unsigned long long ed = warp_sum(cnt.edges);
     const unsigned long long pr = warp_sum((unsigned long long)cnt.processed);
