@@ -166,6 +166,29 @@ rak_status rak_graph_step(rak_ctx *ctx, rak_graph *gr, const rak_options *o, int
 rak_status rak_modularity_f64(rak_ctx *ctx, const rak_csr *g, const uint32_t *membership,
                               double *q);
 
+/* ---- a run that allocates no device memory ------------------------------------------------ */
+/* Size of the fixed device array rak_lowmem_cuda_noalloc works in. Every GPU that loads the
+ * library holds this many bytes until the process exits. */
+#define RAK_NOALLOC_SCRATCH_BYTES (64u << 20)
+
+/* No counterpart in the reference (its runs allocate and free their buffers, inc/rakLowmemCuda.hxx
+ * :570-605). For callers that cannot call cudaMalloc -- e.g. a process whose device memory is
+ * already held by a framework's pooling allocator, or a latency-critical loop that must not pay
+ * cudaMalloc/cudaFree's device synchronisation -- this runs rak_lowmem_cuda on a device-located
+ * graph with every working buffer (flags, plan and its sort space, split-vertex tables and
+ * partial sketches, counters) carved from one file-scope device array of
+ * RAK_NOALLOC_SCRATCH_BYTES; it calls no cudaMalloc, cudaFree or allocating library routine.
+ * g, q (may be NULL), o->initial_flags (may be NULL) and membership are device pointers; work is
+ * issued on `stream` (a cudaStream_t, NULL = legacy default stream) of `device`.
+ * Graphs whose buffers exceed the array (roughly 20 bytes per vertex, plus 8*slots bytes per
+ * split chunk) return RAK_ERR_OUT_OF_MEMORY with res->peak_device_bytes set to the bytes needed.
+ * The first call on a device looks the array up on that device (make it before any stream
+ * capture). All calls share the array and it keeps the last call's contents; each call clears
+ * what must start at zero, and calls that overlap on the GPU race on it. Times in res are host
+ * wall-clock (no CUDA events are created). */
+rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const rak_csr *g, const uint32_t *q,
+                                   const rak_options *o, uint32_t *membership, rak_result *res);
+
 /* ---- synthetic graphs (host, deterministic; for tests and benchmarks) -------------------- */
 /* A host CSR allocated by the library; free with rak_host_csr_free. */
 typedef struct rak_host_csr {

@@ -82,6 +82,9 @@ _sig("rak_graph_device_bytes", C.c_uint64, P)
 _sig("rak_graph_run", C.c_int, P, P, P, C.POINTER(rak_options), P, C.POINTER(rak_result))
 _sig("rak_graph_step", C.c_int, P, P, C.POINTER(rak_options), C.c_int, P, P, P, P, C.POINTER(C.c_uint64))
 _sig("rak_modularity_f64", C.c_int, P, C.POINTER(rak_csr), P, C.POINTER(C.c_double))
+_sig("rak_lowmem_cuda_noalloc", C.c_int, C.c_int, P, C.POINTER(rak_csr), P, C.POINTER(rak_options), P,
+     C.POINTER(rak_result))
+NOALLOC_SCRATCH_BYTES = 64 << 20
 _sig("rak_gen_rmat", C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64,
      C.c_float, C.c_float, C.c_int, C.POINTER(rak_host_csr))
 _sig("rak_gen_sbm", C.c_int, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_uint64, C.c_int,
@@ -307,6 +310,18 @@ class Context:
         q = C.c_double(math.nan)
         _check(_lib.rak_modularity_f64(self._c, C.byref(c), mp, C.byref(q)), self._c)
         return q.value
+
+
+def lowmem_noalloc(device: int, stream_ptr: Optional[int], csr: rak_csr, membership, q=None, **opts) -> Result:
+    """rak_lowmem_cuda_noalloc: a run on a device-located csr that allocates no device memory
+    (working buffers come from the library's fixed device array of NOALLOC_SCRATCH_BYTES)."""
+    o = options(**opts)
+    r = rak_result()
+    st = _lib.rak_lowmem_cuda_noalloc(device, stream_ptr, C.byref(csr), _ptr(q), C.byref(o), membership.data_ptr(),
+                                       C.byref(r))
+    if st != 0:
+        raise RakError(st, f"needs {r.peak_device_bytes} bytes of scratch" if st == 3 else "")
+    return Result.of(r)
 
 
 class ResidentGraph:
