@@ -267,9 +267,12 @@ def main():
     gpu_id = torch.cuda.get_device_properties(local).uuid
     gpu_id = f"GPU-{gpu_id}" if gpu_id else local
     with ClockSampler(gpu_id) as clk:
+        host_ms = []
         ev0.record(stream)
         for _ in range(args.steps):
+            h0 = time.perf_counter()
             results.append(rg.run(membership, **opts))
+            host_ms.append(1e3 * (time.perf_counter() - h0))
         ev1.record(stream)
         barrier()
     elapsed = ev0.elapsed_time(ev1) / 1e3
@@ -362,6 +365,7 @@ def main():
                         "processed_vertices_per_step": last.processed_vertices,
                         "moved_vertices_per_step": last.moved_vertices, "loop_ms": last.loop_ms,
                         "time_ms": last.time_ms, "modularity": res_q.modularity,
+                        "host_ms_per_step": [round(x, 2) for x in host_ms],
                         "memory_gb": last.memory_gb, "plan_ms": last.plan_ms,
                         "peak_device_bytes": res_q.peak_device_bytes}}
         print(json.dumps(line), flush=True)

@@ -28,59 +28,7 @@ struct rak_ctx {
   std::string err;
 };
 
-struct rak_graph {
-  rak_ctx *ctx = nullptr;
-  int64_t n = 0, m = 0;
-  bool off64 = false;
-  bool owns = false;  // graph arrays copied by us (freed on destroy)
-  const void *off = nullptr;
-  const uint32_t *tgt = nullptr;
-  const float *wt = nullptr;
-  rak::Layout ly{0, 0, 0};
-  uint32_t *order = nullptr;
-  uint32_t *chunk_hub = nullptr;
-  int64_t *hub_first = nullptr;
-  int64_t nhub = 0, nchunks = 0;
-  rak::Regions rg{};
-  uint64_t graph_bytes = 0, plan_bytes = 0;
-  float plan_ms = 0, h2d_ms = 0;
-};
-
-namespace {
-
-using rak::Layout;
-
-void set_err(rak_ctx *ctx, const char *fmt, ...) {
-  if (!ctx) return;
-  char buf[512];
-  va_list ap;
-  va_start(ap, fmt);
-  vsnprintf(buf, sizeof(buf), fmt, ap);
-  va_end(ap);
-  ctx->err = buf;
-}
-
-rak_status from_cuda(rak_ctx *ctx, cudaError_t e, const char *what) {
-  if (e == cudaSuccess) return RAK_OK;
-  set_err(ctx, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
-  if (e == cudaErrorMemoryAllocation) {
-    cudaGetLastError();  // not sticky: clear it
-    return RAK_ERR_OUT_OF_MEMORY;
-  }
-  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return RAK_ERR_NO_DEVICE;
-  return RAK_ERR_CUDA;
-}
-
-#define RAK_TRY(ctx, expr)                                         \
-  do {                                                             \
-    rak_status _s = from_cuda((ctx), (expr), #expr);               \
-    if (_s != RAK_OK) return _s;                                   \
-  } while (0)
-#define RAK_CHECK(expr)            \
-  do {                             \
-    rak_status _s = (expr);        \
-    if (_s != RAK_OK) return _s;   \
-  } while (0)
+namespace rak_host_detail {
 
 // Device allocation that frees itself, with byte accounting for peak_device_bytes.
 struct Tracker {
@@ -113,6 +61,81 @@ struct DevBuf {
   }
   template <class T> T *as() const { return static_cast<T *>(p); }
 };
+
+// Per-run device buffers, kept by a resident graph and reused while large enough.
+struct RunBufs {
+  DevBuf vcom1, aff0, aff1, arrive, claim, moved, skk, skw, stats, rs;
+  uint64_t bytes() const {
+    return vcom1.bytes + aff0.bytes + aff1.bytes + arrive.bytes + claim.bytes + moved.bytes + skk.bytes +
+           skw.bytes + stats.bytes + rs.bytes;
+  }
+};
+
+}  // namespace rak_host_detail
+
+struct rak_graph {
+  rak_ctx *ctx = nullptr;
+  int64_t n = 0, m = 0;
+  bool off64 = false;
+  bool owns = false;  // graph arrays copied by us (freed on destroy)
+  const void *off = nullptr;
+  const uint32_t *tgt = nullptr;
+  const float *wt = nullptr;
+  rak::Layout ly{0, 0, 0};
+  uint32_t *order = nullptr;
+  uint32_t *chunk_hub = nullptr;
+  int64_t *hub_first = nullptr;
+  int64_t nhub = 0, nchunks = 0;
+  rak::Regions rg{};
+  uint64_t graph_bytes = 0, plan_bytes = 0;
+  float plan_ms = 0, h2d_ms = 0;
+  rak_host_detail::RunBufs bufs;  // run buffers reused across runs
+};
+
+namespace {
+
+using rak::Layout;
+using rak_host_detail::DevBuf;
+using rak_host_detail::RunBufs;
+using rak_host_detail::Tracker;
+
+// Reuses a cached buffer when it is large enough (untracked: it outlives the call).
+cudaError_t ensure(DevBuf &d, size_t bytes) {
+  if (d.p && d.bytes >= bytes) return cudaSuccess;
+  return d.alloc(bytes, nullptr);
+}
+
+void set_err(rak_ctx *ctx, const char *fmt, ...) {
+  if (!ctx) return;
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  ctx->err = buf;
+}
+
+rak_status from_cuda(rak_ctx *ctx, cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return RAK_OK;
+  set_err(ctx, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();  // not sticky: clear it
+    return RAK_ERR_OUT_OF_MEMORY;
+  }
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return RAK_ERR_NO_DEVICE;
+  return RAK_ERR_CUDA;
+}
+
+#define RAK_TRY(ctx, expr)                                         \
+  do {                                                             \
+    rak_status _s = from_cuda((ctx), (expr), #expr);               \
+    if (_s != RAK_OK) return _s;                                   \
+  } while (0)
+#define RAK_CHECK(expr)            \
+  do {                             \
+    rak_status _s = (expr);        \
+    if (_s != RAK_OK) return _s;   \
+  } while (0)
 
 struct Events {
   cudaEvent_t e[6] = {};
@@ -333,15 +356,6 @@ rak_status graph_create(rak_ctx *ctx, const rak_csr *g, const Resolved &r, Track
   return RAK_OK;
 }
 
-// Per-run device buffers.
-struct RunBufs {
-  DevBuf vcom1, aff0, aff1, arrive, claim, moved, skk, skw, stats, rs;
-  uint64_t bytes() const {
-    return vcom1.bytes + aff0.bytes + aff1.bytes + arrive.bytes + claim.bytes + moved.bytes + skk.bytes +
-           skw.bytes + stats.bytes + rs.bytes;
-  }
-};
-
 // The complete run on a resident graph; labels end up in vcom0 (caller-provided, n entries).
 rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const uint8_t *flags,
                         const Resolved &r, uint32_t *vcom0, Tracker *tr, rak_result *res) {
@@ -350,20 +364,21 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
   const int64_t n = gr->n;
   const bool sync = r.mode != RAK_MODE_ASYNC;
   const int iters = std::max(r.iters, 1);
-  RunBufs b;
-  RAK_TRY(ctx, b.aff0.alloc(size_t(n) + 16, tr));
+  RunBufs &b = gr->bufs;
+  RAK_TRY(ctx, ensure(b.aff0, size_t(n) + 16));
   if (sync) {
-    RAK_TRY(ctx, b.vcom1.alloc(size_t(n) * 4 + 16, tr));
-    RAK_TRY(ctx, b.aff1.alloc(size_t(n) + 16, tr));
+    RAK_TRY(ctx, ensure(b.vcom1, size_t(n) * 4 + 16));
+    RAK_TRY(ctx, ensure(b.aff1, size_t(n) + 16));
   }
   const size_t nh = size_t(std::max<int64_t>(gr->nhub, 1)), nc = size_t(std::max<int64_t>(gr->nchunks, 1));
-  RAK_TRY(ctx, b.arrive.alloc(nh * 4, tr));
-  RAK_TRY(ctx, b.claim.alloc(nh * 4, tr));
-  RAK_TRY(ctx, b.moved.alloc(nh * 4, tr));
-  RAK_TRY(ctx, b.skk.alloc(nc * size_t(r.slots) * 4, tr));
-  RAK_TRY(ctx, b.skw.alloc(nc * size_t(r.slots) * 4, tr));
-  RAK_TRY(ctx, b.stats.alloc(size_t(iters) * rak::STATS_STRIDE * 8, tr));
-  RAK_TRY(ctx, b.rs.alloc(sizeof(rak::RunStateHost), tr));
+  RAK_TRY(ctx, ensure(b.arrive, nh * 4));
+  RAK_TRY(ctx, ensure(b.claim, nh * 4));
+  RAK_TRY(ctx, ensure(b.moved, nh * 4));
+  RAK_TRY(ctx, ensure(b.skk, nc * size_t(r.slots) * 4));
+  RAK_TRY(ctx, ensure(b.skw, nc * size_t(r.slots) * 4));
+  RAK_TRY(ctx, ensure(b.stats, size_t(iters) * rak::STATS_STRIDE * 8));
+  RAK_TRY(ctx, ensure(b.rs, sizeof(rak::RunStateHost)));
+  if (tr) tr->add(b.bytes());
 
   rak::LpaArgs a{};
   a.off = gr->off; a.tgt = gr->tgt; a.wt = gr->wt; a.n = n;
