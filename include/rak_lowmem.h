@@ -166,6 +166,44 @@ rak_status rak_graph_step(rak_ctx *ctx, rak_graph *gr, const rak_options *o, int
 rak_status rak_modularity_f64(rak_ctx *ctx, const rak_csr *g, const uint32_t *membership,
                               double *q);
 
+/* ---- batches of independent graphs ------------------------------------------------------- */
+/* Many graphs concatenated into one CSR: graph g owns vertices [graph_offsets[g],
+ * graph_offsets[g+1]); offsets index the concatenated targets/weights; targets are ids LOCAL to the
+ * edge's own graph. Replaces a loop of rakLowmemStaticCuda calls, one per graph (main.cxx:84-92). */
+typedef struct rak_batch_csr {
+  int64_t graphs;                /* number of graphs */
+  int64_t n;                     /* total vertices, == graph_offsets[graphs], < 2^31 */
+  int64_t m;                     /* total directed edges, == offsets[n] */
+  int32_t location;              /* rak_location of every array */
+  int32_t reserved;
+  const int64_t *graph_offsets;  /* graphs+1 */
+  const int64_t *offsets;        /* n+1 */
+  const uint32_t *targets;       /* m local ids */
+  const float *weights;          /* m, or NULL for unit weights */
+} rak_batch_csr;
+
+typedef struct rak_batch rak_batch;
+
+/* Device-resident copy of a batch (or a binding of a device-located one) with its plan. */
+rak_status rak_batch_create(rak_ctx *ctx, const rak_batch_csr *b, const rak_options *o, rak_batch **out);
+rak_status rak_batch_destroy(rak_batch *b);
+/* Enqueues one complete run of every graph on the context's stream -- a single persistent launch
+ * in which each graph iterates until its own convergence test passes -- and returns without
+ * waiting. q (local initial labels, may be NULL) and membership (local labels, written) are device
+ * pointers with n entries. The sequence makes no host round trip, so it can be captured into a
+ * CUDA graph. */
+rak_status rak_batch_launch(rak_ctx *ctx, rak_batch *b, const uint32_t *q, const rak_options *o,
+                            uint32_t *membership);
+/* Waits for the last launch; iterations (host, `graphs` entries, may be NULL) receives each graph's
+ * iteration count, total (may be NULL) the counters summed over graphs. */
+rak_status rak_batch_results(rak_ctx *ctx, rak_batch *b, int32_t *iterations, rak_result *total);
+/* Captures rak_batch_launch(q, o, membership) into a CUDA graph kept by the batch, and replays it. */
+rak_status rak_batch_capture(rak_ctx *ctx, rak_batch *b, const uint32_t *q, const rak_options *o,
+                             uint32_t *membership);
+rak_status rak_batch_replay(rak_ctx *ctx, rak_batch *b);
+/* FP64 modularity of every graph (membership: device, local labels); q: host, `graphs` entries. */
+rak_status rak_batch_modularity_f64(rak_ctx *ctx, rak_batch *b, const uint32_t *membership, double *q);
+
 /* ---- a run that allocates no device memory ------------------------------------------------ */
 /* Size of the fixed device array rak_lowmem_cuda_noalloc works in. Every GPU that loads the
  * library holds this many bytes until the process exits. */

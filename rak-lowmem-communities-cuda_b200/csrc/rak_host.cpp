@@ -75,6 +75,7 @@ struct RunBufs {
 
 struct rak_graph {
   rak_ctx *ctx = nullptr;
+  int device = 0;                   // kept here: the context may be destroyed first
   int64_t n = 0, m = 0;
   bool off64 = false;
   bool owns = false;  // graph arrays copied by us (freed on destroy)
@@ -90,6 +91,18 @@ struct rak_graph {
   uint64_t graph_bytes = 0, plan_bytes = 0;
   float plan_ms = 0, h2d_ms = 0;
   rak_host_detail::RunBufs bufs;  // run buffers reused across runs
+};
+
+struct rak_batch {
+  rak_ctx *ctx = nullptr;
+  int device = 0;
+  rak_graph *g = nullptr;           // the concatenated CSR (64-bit offsets) and its plan
+  int64_t ngraphs = 0;
+  rak_host_detail::DevBuf vbase, gid, vcom0, gdone, giters, gchanged, running;
+  int last_iters = 0;               // max_iterations of the last launch
+  bool last_sync = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
 };
 
 namespace {
@@ -306,6 +319,7 @@ rak_status graph_create(rak_ctx *ctx, const rak_csr *g, const Resolved &r, Track
   auto *gr = new (std::nothrow) rak_graph();
   if (!gr) return RAK_ERR_OUT_OF_MEMORY;
   gr->ctx = ctx;
+  gr->device = ctx->device;
   gr->n = g->n;
   gr->m = g->m;
   gr->off64 = g->offset_bits == 64;
@@ -537,6 +551,7 @@ rak_status rak_ctx_set_stream(rak_ctx *ctx, void *stream) {
 const char *rak_ctx_last_error(const rak_ctx *ctx) { return ctx ? ctx->err.c_str() : ""; }
 
 rak_status rak_graph_create(rak_ctx *ctx, const rak_csr *g, const rak_options *o, rak_graph **out) {
+  cudaGetLastError();  // drop a stale error left by an unrelated failed call
   if (!ctx || !out) return RAK_ERR_INVALID_ARGUMENT;
   Resolved r;
   RAK_CHECK(resolve(ctx, o, &r));
@@ -545,7 +560,7 @@ rak_status rak_graph_create(rak_ctx *ctx, const rak_csr *g, const rak_options *o
 
 rak_status rak_graph_destroy(rak_graph *gr) {
   if (!gr) return RAK_ERR_INVALID_ARGUMENT;
-  if (gr->ctx) cudaSetDevice(gr->ctx->device);
+  cudaSetDevice(gr->device);
   if (gr->owns) {
     cudaFree(const_cast<void *>(gr->off));
     cudaFree(const_cast<uint32_t *>(gr->tgt));
@@ -562,6 +577,7 @@ uint64_t rak_graph_device_bytes(const rak_graph *gr) { return gr ? gr->graph_byt
 
 rak_status rak_graph_run(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const rak_options *o,
                          uint32_t *membership, rak_result *res) {
+  cudaGetLastError();  // drop a stale error left by an unrelated failed call
   if (!ctx || !gr || !membership) return RAK_ERR_INVALID_ARGUMENT;
   Resolved r;
   RAK_CHECK(resolve(ctx, o, &r));
@@ -581,6 +597,7 @@ rak_status rak_graph_run(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const r
 
 rak_status rak_lowmem_cuda(rak_ctx *ctx, const rak_csr *g, const uint32_t *q, const rak_options *o,
                            uint32_t *membership, rak_result *res) {
+  cudaGetLastError();  // drop a stale error left by an unrelated failed call
   if (!ctx || !g || !membership) return RAK_ERR_INVALID_ARGUMENT;
   Resolved r;
   RAK_CHECK(resolve(ctx, o, &r));
@@ -631,6 +648,7 @@ rak_status rak_lowmem_cuda(rak_ctx *ctx, const rak_csr *g, const uint32_t *q, co
 rak_status rak_graph_step(rak_ctx *ctx, rak_graph *gr, const rak_options *o, int iteration,
                           const uint32_t *vcom_prev, const uint8_t *aff_prev, uint32_t *vcom_next,
                           uint8_t *aff_next, uint64_t *changed) {
+  cudaGetLastError();  // drop a stale error left by an unrelated failed call
   if (!ctx || !gr || !vcom_prev || !aff_prev || !vcom_next || !aff_next) return RAK_ERR_INVALID_ARGUMENT;
   Resolved r;
   RAK_CHECK(resolve(ctx, o, &r));
@@ -684,6 +702,7 @@ rak_status rak_graph_step(rak_ctx *ctx, rak_graph *gr, const rak_options *o, int
 }
 
 rak_status rak_modularity_f64(rak_ctx *ctx, const rak_csr *g, const uint32_t *membership, double *q) {
+  cudaGetLastError();  // drop a stale error left by an unrelated failed call
   if (!ctx || !g || !membership || !q) return RAK_ERR_INVALID_ARGUMENT;
   RAK_CHECK(check_csr_shape(ctx, g));
   RAK_TRY(ctx, cudaSetDevice(ctx->device));
@@ -741,6 +760,256 @@ rak_status rak_plan_summary_host(const rak_csr *g, const rak_options *o, int64_t
     else counts[6 - reg]++;  // region 5 (G=2) -> 1, ..., region 1 (G=32) -> 5
   }
   if (hub_chunks) *hub_chunks = ch;
+  return RAK_OK;
+}
+
+}  // extern "C"
+
+// ---- batches of graphs ----------------------------------------------------------------------
+
+namespace {
+
+rak_status batch_prepare(rak_ctx *ctx, rak_batch *b, const Resolved &r) {
+  rak_graph *gr = b->g;
+  if (!same_layout(gr->ly, r.ly)) RAK_CHECK(build_plan(ctx, gr, r.ly, nullptr));
+  const int64_t n = gr->n, G = b->ngraphs;
+  const bool sync = r.mode != RAK_MODE_ASYNC;
+  const int iters = std::max(r.iters, 1);
+  RunBufs &rb = gr->bufs;
+  RAK_TRY(ctx, ensure(rb.aff0, size_t(n) + 16));
+  if (sync) {
+    RAK_TRY(ctx, ensure(rb.vcom1, size_t(n) * 4 + 16));
+    RAK_TRY(ctx, ensure(rb.aff1, size_t(n) + 16));
+  }
+  const size_t nh = size_t(std::max<int64_t>(gr->nhub, 1)), nc = size_t(std::max<int64_t>(gr->nchunks, 1));
+  RAK_TRY(ctx, ensure(rb.arrive, nh * 4));
+  RAK_TRY(ctx, ensure(rb.claim, nh * 4));
+  RAK_TRY(ctx, ensure(rb.moved, nh * 4));
+  RAK_TRY(ctx, ensure(rb.skk, nc * size_t(r.slots) * 4));
+  RAK_TRY(ctx, ensure(rb.skw, nc * size_t(r.slots) * 4));
+  RAK_TRY(ctx, ensure(rb.stats, size_t(iters) * rak::STATS_STRIDE * 8));
+  RAK_TRY(ctx, ensure(rb.rs, sizeof(rak::RunStateHost)));
+  RAK_TRY(ctx, ensure(b->vcom0, size_t(n) * 4 + 16));
+  RAK_TRY(ctx, ensure(b->gdone, size_t(G) + 16));
+  RAK_TRY(ctx, ensure(b->giters, size_t(G) * 4 + 16));
+  RAK_TRY(ctx, ensure(b->gchanged, size_t(G) * 16 + 16));
+  RAK_TRY(ctx, ensure(b->running, size_t(iters) * 4 + 16));
+  return RAK_OK;
+}
+
+// Enqueues the whole run; buffers must already be prepared (no allocation here, so the sequence
+// is capturable).
+rak_status batch_enqueue(rak_ctx *ctx, rak_batch *b, const uint32_t *q, const Resolved &r, uint32_t *membership) {
+  rak_graph *gr = b->g;
+  RunBufs &rb = gr->bufs;
+  cudaStream_t st = ctx->stream;
+  const int64_t n = gr->n, G = b->ngraphs;
+  const bool sync = r.mode != RAK_MODE_ASYNC;
+  const int iters = std::max(r.iters, 1);
+  RAK_TRY(ctx, cudaMemsetAsync(rb.arrive.p, 0, rb.arrive.bytes, st));
+  RAK_TRY(ctx, cudaMemsetAsync(rb.claim.p, 0, rb.claim.bytes, st));
+  RAK_TRY(ctx, cudaMemsetAsync(rb.moved.p, 0xFF, rb.moved.bytes, st));
+  RAK_TRY(ctx, cudaMemsetAsync(rb.stats.p, 0, size_t(iters) * rak::STATS_STRIDE * 8, st));
+  RAK_TRY(ctx, cudaMemsetAsync(rb.rs.p, 0, sizeof(rak::RunStateHost), st));
+  RAK_TRY(ctx, cudaMemsetAsync(b->gdone.p, 0, size_t(G) + 16, st));
+  RAK_TRY(ctx, cudaMemsetAsync(b->giters.p, 0, size_t(G) * 4 + 16, st));
+  RAK_TRY(ctx, cudaMemsetAsync(b->gchanged.p, 0, size_t(G) * 16 + 16, st));
+  RAK_TRY(ctx, cudaMemsetAsync(b->running.p, 0, size_t(iters) * 4 + 16, st));
+  uint32_t *v1 = sync ? rb.vcom1.as<uint32_t>() : nullptr;
+  RAK_TRY(ctx, rak::launch_batch_init(b->vcom0.as<uint32_t>(), v1, q, b->gid.as<uint32_t>(), b->vbase.as<int64_t>(), n, st));
+  RAK_TRY(ctx, rak::launch_init_flags(rb.aff0.as<uint8_t>(), sync ? rb.aff1.as<uint8_t>() : nullptr, nullptr, n, st));
+  if (r.iters > 0) {
+    rak::LpaArgs a{};
+    a.off = gr->off; a.tgt = gr->tgt; a.wt = gr->wt; a.n = n;
+    a.order = gr->order; a.rg = gr->rg;
+    a.chunk_hub = gr->chunk_hub; a.hub_first = gr->hub_first; a.hub_chunk = gr->ly.hub_chunk; a.nchunks = gr->nchunks;
+    a.vcom0 = b->vcom0.as<uint32_t>(); a.vcom1 = v1; a.aff0 = rb.aff0.as<uint8_t>(); a.aff1 = sync ? rb.aff1.as<uint8_t>() : nullptr;
+    a.hub_arrive = rb.arrive.as<uint32_t>(); a.hub_claim = rb.claim.as<uint32_t>(); a.hub_moved = rb.moved.as<int32_t>();
+    a.sk_keys = rb.skk.as<uint32_t>(); a.sk_wts = rb.skw.as<float>();
+    a.stats = rb.stats.as<unsigned long long>(); a.rs = rb.rs.p;
+    a.gid = b->gid.as<uint32_t>(); a.vbase = b->vbase.as<int64_t>(); a.gdone = b->gdone.as<uint8_t>();
+    a.giters = b->giters.as<int32_t>(); a.gchanged = b->gchanged.as<unsigned long long>();
+    a.running = b->running.as<unsigned int>(); a.ngraphs = G;
+    a.iters = r.iters; a.start_iter = r.start; a.tolerance = r.tol; a.pickless_step = r.pickless;
+    a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.timeout_ns = 20LL * 1000 * 1000 * 1000;
+    int grid = 0;
+    RAK_TRY(ctx, rak::launch_lpa(a, r.slots, r.mode, true, st, &grid, true));
+  }
+  RAK_TRY(ctx, rak::launch_batch_finish(b->vcom0.as<uint32_t>(), r.iters > 0 ? v1 : nullptr, rb.rs.p,
+                                        b->gid.as<uint32_t>(), b->vbase.as<int64_t>(), n, membership, st));
+  b->last_iters = iters;
+  b->last_sync = sync;
+  return RAK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+rak_status rak_batch_create(rak_ctx *ctx, const rak_batch_csr *bc, const rak_options *o, rak_batch **out) {
+  cudaGetLastError();  // drop a stale error left by an unrelated failed call
+  if (!ctx || !bc || !out) return RAK_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (bc->graphs < 0 || !bc->graph_offsets) { set_err(ctx, "bad graph count or offsets"); return RAK_ERR_INVALID_ARGUMENT; }
+  Resolved r;
+  RAK_CHECK(resolve(ctx, o, &r));
+  RAK_TRY(ctx, cudaSetDevice(ctx->device));
+  rak_csr c{};
+  c.n = bc->n; c.m = bc->m; c.offset_bits = 64; c.location = bc->location;
+  c.offsets = bc->offsets; c.targets = bc->targets; c.weights = bc->weights;
+  Resolved rn = r;
+  rn.validate = 0;  // the batch rules (local target ids) are checked below
+  if (r.validate && bc->location == RAK_HOST) {
+    const int64_t *go = bc->graph_offsets, *off = bc->offsets;
+    if (check_csr_shape(ctx, &c) != RAK_OK) return RAK_ERR_INVALID_ARGUMENT;
+    bool ok = go[0] == 0 && go[bc->graphs] == bc->n && off[0] == 0 && off[bc->n] == bc->m;
+    for (int64_t gi = 0; ok && gi < bc->graphs; ++gi) {
+      if (go[gi] > go[gi + 1]) { ok = false; break; }
+      const int64_t ng = go[gi + 1] - go[gi];
+      for (int64_t u = go[gi]; ok && u < go[gi + 1]; ++u) {
+        if (off[u] > off[u + 1]) ok = false;
+        for (int64_t e = off[u]; ok && e < off[u + 1]; ++e) ok = int64_t(bc->targets[e]) < ng;
+      }
+    }
+    if (!ok) { set_err(ctx, "invalid batch CSR (host check)"); return RAK_ERR_INVALID_CSR; }
+  }
+  auto *b = new (std::nothrow) rak_batch();
+  if (!b) return RAK_ERR_OUT_OF_MEMORY;
+  b->ctx = ctx;
+  b->device = ctx->device;
+  b->ngraphs = bc->graphs;
+  struct Fail { rak_batch *b; bool armed = true; ~Fail() { if (armed) rak_batch_destroy(b); } } fail{b};
+  RAK_CHECK(graph_create(ctx, &c, rn, nullptr, &b->g));
+  const size_t gbytes = size_t(bc->graphs + 1) * 8;
+  RAK_TRY(ctx, b->vbase.alloc(gbytes, nullptr));
+  RAK_TRY(ctx, cudaMemcpyAsync(b->vbase.p, bc->graph_offsets, gbytes,
+                               bc->location == RAK_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, ctx->stream));
+  RAK_TRY(ctx, b->gid.alloc(size_t(std::max<int64_t>(bc->n, 1)) * 4, nullptr));
+  RAK_TRY(ctx, rak::launch_batch_gid(b->vbase.as<int64_t>(), bc->graphs, b->gid.as<uint32_t>(), ctx->stream));
+  if (r.validate && bc->location == RAK_DEVICE) {
+    DevBuf bad;
+    unsigned int hbad = 0;
+    RAK_TRY(ctx, bad.alloc(4, nullptr));
+    RAK_TRY(ctx, cudaMemsetAsync(bad.p, 0, 4, ctx->stream));
+    RAK_TRY(ctx, rak::launch_batch_validate(b->vbase.as<int64_t>(), bc->graphs, bc->n, static_cast<const int64_t *>(b->g->off),
+                                            b->g->tgt, b->gid.as<uint32_t>(), bad.as<unsigned int>(), ctx->stream));
+    RAK_TRY(ctx, cudaMemcpyAsync(&hbad, bad.p, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    RAK_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (hbad) { set_err(ctx, "invalid batch CSR (device check)"); return RAK_ERR_INVALID_CSR; }
+  }
+  RAK_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  fail.armed = false;
+  *out = b;
+  return RAK_OK;
+}
+
+rak_status rak_batch_destroy(rak_batch *b) {
+  if (!b) return RAK_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(b->device);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->g) rak_graph_destroy(b->g);
+  delete b;
+  return RAK_OK;
+}
+
+rak_status rak_batch_launch(rak_ctx *ctx, rak_batch *b, const uint32_t *q, const rak_options *o, uint32_t *membership) {
+  cudaGetLastError();  // drop a stale error left by an unrelated failed call
+  if (!ctx || !b || !membership) return RAK_ERR_INVALID_ARGUMENT;
+  Resolved r;
+  RAK_CHECK(resolve(ctx, o, &r));
+  RAK_TRY(ctx, cudaSetDevice(ctx->device));
+  RAK_CHECK(batch_prepare(ctx, b, r));
+  return batch_enqueue(ctx, b, q, r, membership);
+}
+
+rak_status rak_batch_results(rak_ctx *ctx, rak_batch *b, int32_t *iterations, rak_result *total) {
+  cudaGetLastError();  // drop a stale error left by an unrelated failed call
+  if (!ctx || !b) return RAK_ERR_INVALID_ARGUMENT;
+  RAK_TRY(ctx, cudaSetDevice(ctx->device));
+  RAK_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  RunBufs &rb = b->g->bufs;
+  rak::RunStateHost hs{};
+  if (!rb.rs.p) { set_err(ctx, "no launch yet"); return RAK_ERR_INVALID_ARGUMENT; }
+  RAK_TRY(ctx, cudaMemcpy(&hs, rb.rs.p, sizeof(hs), cudaMemcpyDeviceToHost));
+  if (hs.error) { set_err(ctx, "device-side wait gave up (status %u)", hs.error); return rak_status(hs.error); }
+  if (iterations && b->ngraphs > 0)
+    RAK_TRY(ctx, cudaMemcpy(iterations, b->giters.p, size_t(b->ngraphs) * 4, cudaMemcpyDeviceToHost));
+  if (total) {
+    std::memset(total, 0, sizeof(*total));
+    total->modularity = std::numeric_limits<double>::quiet_NaN();
+    std::vector<unsigned long long> st(size_t(b->last_iters) * rak::STATS_STRIDE);
+    RAK_TRY(ctx, cudaMemcpy(st.data(), rb.stats.p, st.size() * 8, cudaMemcpyDeviceToHost));
+    const int done = int(std::min<unsigned>(hs.iterations, unsigned(b->last_iters)));
+    total->iterations = done;
+    for (int i = 0; i < done; ++i) {
+      const unsigned long long *x = &st[size_t(i) * rak::STATS_STRIDE];
+      total->traversed_edges += x[rak::STAT_EDGES];
+      total->processed_vertices += x[rak::STAT_PROCESSED];
+      total->moved_vertices += x[rak::STAT_CHANGED];
+      total->moved_edges += x[rak::STAT_MOVED_EDGES];
+    }
+    total->changed_last = done > 0 ? st[size_t(done - 1) * rak::STATS_STRIDE + rak::STAT_CHANGED] : 0;
+    total->plan_ms = b->g->plan_ms;
+    const uint64_t bytes = b->g->graph_bytes + b->g->plan_bytes + rb.bytes() + b->vbase.bytes + b->gid.bytes +
+                           b->vcom0.bytes + b->gdone.bytes + b->giters.bytes + b->gchanged.bytes + b->running.bytes;
+    total->peak_device_bytes = bytes;
+    total->memory_gb = float(double(bytes - b->g->graph_bytes) / (1024.0 * 1024.0 * 1024.0));
+  }
+  return RAK_OK;
+}
+
+rak_status rak_batch_capture(rak_ctx *ctx, rak_batch *b, const uint32_t *q, const rak_options *o, uint32_t *membership) {
+  cudaGetLastError();  // drop a stale error left by an unrelated failed call
+  if (!ctx || !b || !membership) return RAK_ERR_INVALID_ARGUMENT;
+  Resolved r;
+  RAK_CHECK(resolve(ctx, o, &r));
+  RAK_TRY(ctx, cudaSetDevice(ctx->device));
+  RAK_CHECK(batch_prepare(ctx, b, r));  // allocations happen before the capture
+  if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+  if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+  RAK_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  rak_status s = batch_enqueue(ctx, b, q, r, membership);
+  cudaGraph_t gph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(ctx->stream, &gph);
+  if (s != RAK_OK) { if (gph) cudaGraphDestroy(gph); return s; }
+  RAK_TRY(ctx, e);
+  b->graph = gph;
+  RAK_TRY(ctx, cudaGraphInstantiate(&b->exec, gph, 0));
+  return RAK_OK;
+}
+
+rak_status rak_batch_replay(rak_ctx *ctx, rak_batch *b) {
+  cudaGetLastError();  // drop a stale error left by an unrelated failed call
+  if (!ctx || !b || !b->exec) return RAK_ERR_INVALID_ARGUMENT;
+  RAK_TRY(ctx, cudaSetDevice(ctx->device));
+  RAK_TRY(ctx, cudaGraphLaunch(b->exec, ctx->stream));
+  return RAK_OK;
+}
+
+rak_status rak_batch_modularity_f64(rak_ctx *ctx, rak_batch *b, const uint32_t *membership, double *q) {
+  cudaGetLastError();  // drop a stale error left by an unrelated failed call
+  if (!ctx || !b || !membership || !q) return RAK_ERR_INVALID_ARGUMENT;
+  RAK_TRY(ctx, cudaSetDevice(ctx->device));
+  const int64_t n = b->g->n, G = b->ngraphs;
+  DevBuf ctot, gs;
+  RAK_TRY(ctx, ctot.alloc(size_t(std::max<int64_t>(n, 1)) * 8, nullptr));
+  RAK_TRY(ctx, gs.alloc(size_t(3 * G + 1) * 8, nullptr));
+  RAK_TRY(ctx, cudaMemsetAsync(ctot.p, 0, ctot.bytes, ctx->stream));
+  RAK_TRY(ctx, cudaMemsetAsync(gs.p, 0, gs.bytes, ctx->stream));
+  double *gin = gs.as<double>(), *gtot = gin + G, *gsq = gtot + G, *bad = gsq + G;
+  if (n > 0)
+    RAK_TRY(ctx, rak::launch_batch_modularity(static_cast<const int64_t *>(b->g->off), b->g->tgt, b->g->wt,
+                                              b->gid.as<uint32_t>(), b->vbase.as<int64_t>(), n, membership,
+                                              ctot.as<double>(), gin, gtot, gsq, bad, ctx->stream));
+  std::vector<double> h(size_t(3 * G + 1));
+  RAK_TRY(ctx, cudaMemcpyAsync(h.data(), gs.p, h.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  RAK_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (h[size_t(3 * G)] > 0) { set_err(ctx, "membership holds labels beyond their graph"); return RAK_ERR_INVALID_ARGUMENT; }
+  for (int64_t gi = 0; gi < G; ++gi) {
+    const double in = h[size_t(gi)], tot = h[size_t(G + gi)], sq = h[size_t(2 * G + gi)];
+    q[gi] = tot > 0 ? in / tot - sq / (tot * tot) : 0.0;
+  }
   return RAK_OK;
 }
 

@@ -76,6 +76,14 @@ struct LpaArgs {
   float *sk_wts;               // per chunk: slots weights
   unsigned long long *stats;   // per iteration, STATS_STRIDE slots (STAT_* below)
   void *rs;                    // RunState
+  // Batches of independent graphs (BATCH kernels): targets are ids local to their graph.
+  const uint32_t *gid;          // per vertex: index of its graph
+  const int64_t *vbase;         // per graph: first vertex (ngraphs+1 entries)
+  uint8_t *gdone;               // per graph: converged (its vertices are no longer processed)
+  int32_t *giters;              // per graph: iterations it ran
+  unsigned long long *gchanged; // 2*ngraphs: vertices changed per graph, this and next iteration
+  unsigned int *running;        // per iteration: graphs still running after it
+  int64_t ngraphs;
   int iters;
   int start_iter;
   double tolerance;
@@ -91,11 +99,13 @@ enum Mode { MODE_ASYNC = 0, MODE_SYNC = 1, MODE_SPLIT = 2 };
 enum Stat { STAT_CHANGED = 0, STAT_EDGES = 1, STAT_PROCESSED = 2, STAT_HUBS_MOVED = 3, STAT_MOVED_EDGES = 4, STAT_WORK = 5 };
 constexpr int STATS_STRIDE = 8;
 
-// Persistent cooperative launch of all iterations; grid chosen from occupancy.
-cudaError_t launch_lpa(const LpaArgs &a, int slots, int mode, bool off64, cudaStream_t st, int *grid_out);
+// Persistent cooperative launch of all iterations; grid chosen from occupancy. `batch` selects the
+// kernels for concatenated batches of graphs (64-bit offsets only).
+cudaError_t launch_lpa(const LpaArgs &a, int slots, int mode, bool off64, cudaStream_t st, int *grid_out,
+                       bool batch = false);
 // Per-slot-count instantiations (rak_lpa_s*.cu).
 template <int S>
-cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, cudaStream_t st, int *grid_out);
+cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, bool batch, cudaStream_t st, int *grid_out);
 
 // Plan and utility kernels (rak_kernels.cu).
 cudaError_t launch_validate(const void *off, bool off64, const uint32_t *tgt, int64_t n, int64_t m,
@@ -111,5 +121,17 @@ cudaError_t launch_hub_degrees(const void *off, bool off64, const uint32_t *orde
 cudaError_t launch_modularity(const void *off, bool off64, const uint32_t *tgt, const float *wt,
                               int64_t n, const uint32_t *labels, double *ctot, double *sums,
                               cudaStream_t st);
+
+// Batches of graphs (rak_kernels.cu).
+cudaError_t launch_batch_gid(const int64_t *vbase, int64_t ngraphs, uint32_t *gid, cudaStream_t st);
+cudaError_t launch_batch_validate(const int64_t *vbase, int64_t ngraphs, int64_t n, const int64_t *off,
+                                  const uint32_t *tgt, const uint32_t *gid, unsigned int *bad, cudaStream_t st);
+cudaError_t launch_batch_init(uint32_t *v0, uint32_t *v1, const uint32_t *q, const uint32_t *gid,
+                              const int64_t *vbase, int64_t n, cudaStream_t st);
+cudaError_t launch_batch_finish(const uint32_t *v0, const uint32_t *v1, const void *rs, const uint32_t *gid,
+                                const int64_t *vbase, int64_t n, uint32_t *membership, cudaStream_t st);
+cudaError_t launch_batch_modularity(const int64_t *off, const uint32_t *tgt, const float *wt, const uint32_t *gid,
+                                    const int64_t *vbase, int64_t n, const uint32_t *labels, double *ctot,
+                                    double *gin, double *gtot, double *gsq, double *bad, cudaStream_t st);
 
 }  // namespace rak

@@ -130,7 +130,121 @@ __global__ void k_mod_square(const double *ctot, int64_t n, double *sums) {
   }
 }
 
+// ---- batches of graphs ------------------------------------------------------------------------
+// gid[u] = graph of vertex u, from the graph vertex offsets.
+__global__ void k_batch_gid(const int64_t *vbase, int64_t ngraphs, uint32_t *gid) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t g = tid; g < ngraphs; g += nt)
+    for (int64_t u = vbase[g]; u < vbase[g + 1]; ++u) gid[u] = uint32_t(g);
+}
+
+// Batch CSR rules: graph offsets non-decreasing from 0 to n, and every target (a local id) below
+// its own graph's vertex count. Violations set *bad.
+__global__ void k_batch_validate(const int64_t *vbase, int64_t ngraphs, int64_t n, const int64_t *off,
+                                 const uint32_t *tgt, const uint32_t *gid, unsigned int *bad) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  if (tid == 0 && (vbase[0] != 0 || vbase[ngraphs] != n)) atomicOr(bad, 1u);
+  for (int64_t g = tid; g < ngraphs; g += nt)
+    if (vbase[g] > vbase[g + 1]) atomicOr(bad, 1u);
+  for (int64_t u = tid; u < n; u += nt) {
+    const uint32_t g = gid[u];
+    const int64_t ng = vbase[g + 1] - vbase[g];
+    for (int64_t e = off[u]; e < off[u + 1]; ++e)
+      if (int64_t(tgt[e]) >= ng) { atomicOr(bad, 2u); break; }
+  }
+}
+
+// Labels at the start of a batch run: global vertex ids, from local initial labels q if given.
+__global__ void k_batch_init(uint32_t *v0, uint32_t *v1, const uint32_t *q, const uint32_t *gid,
+                             const int64_t *vbase, int64_t n) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t u = tid; u < n; u += nt) {
+    const uint32_t c = q ? uint32_t(vbase[gid[u]]) + q[u] : uint32_t(u);
+    v0[u] = c;
+    if (v1) v1[u] = c;
+  }
+}
+
+// Final local labels: the buffer the last iteration wrote (decided on the device from the
+// iteration count, so the launch sequence needs no host round trip), minus the graph's offset.
+__global__ void k_batch_finish(const uint32_t *v0, const uint32_t *v1, const RunState *rs, const uint32_t *gid,
+                               const int64_t *vbase, int64_t n, uint32_t *membership) {
+  const uint32_t *src = (v1 && (rs->iterations & 1u)) ? v1 : v0;
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t u = tid; u < n; u += nt) membership[u] = src[u] - uint32_t(vbase[gid[u]]);
+}
+
+// Per-graph FP64 modularity terms: internal weight and total weight per graph, community totals
+// per global label (ctot), then squared community totals per graph. labels are local.
+__global__ void k_batch_mod_vertex(const int64_t *off, const uint32_t *tgt, const float *wt, const uint32_t *gid,
+                                   const int64_t *vbase, int64_t n, const uint32_t *labels, double *ctot,
+                                   double *gin, double *gtot, double *bad) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5, nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t u = w0; u < n; u += nw) {
+    const uint32_t g = gid[u];
+    const int64_t base = vbase[g], ng = vbase[g + 1] - base;
+    const uint32_t c = labels[u];
+    if (int64_t(c) >= ng) {
+      if (lane == 0) atomicAdd(bad, 1.0);
+      continue;
+    }
+    double kin = 0.0, kt = 0.0;
+    for (int64_t e = off[u] + lane; e < off[u + 1]; e += 32) {
+      const double w = wt ? double(wt[e]) : 1.0;
+      kt += w;
+      if (labels[base + tgt[e]] == c) kin += w;
+    }
+    kin = warp_sum(kin);
+    kt = warp_sum(kt);
+    if (lane == 0 && kt != 0.0) {
+      atomicAdd(ctot + base + c, kt);
+      atomicAdd(gin + g, kin);
+      atomicAdd(gtot + g, kt);
+    }
+  }
+}
+
+__global__ void k_batch_mod_square(const double *ctot, const uint32_t *gid, int64_t n, double *gsq) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t c = tid; c < n; c += nt)
+    if (ctot[c] != 0.0) atomicAdd(gsq + gid[c], ctot[c] * ctot[c]);
+}
+
 }  // namespace
+
+cudaError_t launch_batch_gid(const int64_t *vbase, int64_t ngraphs, uint32_t *gid, cudaStream_t st) {
+  k_batch_gid<<<grid_for(ngraphs), TPB, 0, st>>>(vbase, ngraphs, gid);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_validate(const int64_t *vbase, int64_t ngraphs, int64_t n, const int64_t *off,
+                                  const uint32_t *tgt, const uint32_t *gid, unsigned int *bad, cudaStream_t st) {
+  k_batch_validate<<<grid_for(n > ngraphs ? n : ngraphs, 4), TPB, 0, st>>>(vbase, ngraphs, n, off, tgt, gid, bad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_init(uint32_t *v0, uint32_t *v1, const uint32_t *q, const uint32_t *gid,
+                              const int64_t *vbase, int64_t n, cudaStream_t st) {
+  k_batch_init<<<grid_for(n, 4), TPB, 0, st>>>(v0, v1, q, gid, vbase, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_finish(const uint32_t *v0, const uint32_t *v1, const void *rs, const uint32_t *gid,
+                                const int64_t *vbase, int64_t n, uint32_t *membership, cudaStream_t st) {
+  k_batch_finish<<<grid_for(n, 4), TPB, 0, st>>>(v0, v1, static_cast<const RunState *>(rs), gid, vbase, n, membership);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_modularity(const int64_t *off, const uint32_t *tgt, const float *wt, const uint32_t *gid,
+                                    const int64_t *vbase, int64_t n, const uint32_t *labels, double *ctot,
+                                    double *gin, double *gtot, double *gsq, double *bad, cudaStream_t st) {
+  k_batch_mod_vertex<<<grid_for(n * 32, 4), TPB, 0, st>>>(off, tgt, wt, gid, vbase, n, labels, ctot, gin, gtot, bad);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_batch_mod_square<<<grid_for(n, 4), TPB, 0, st>>>(ctot, gid, n, gsq);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_validate(const void *off, bool off64, const uint32_t *tgt, int64_t n, int64_t m,
                             unsigned int *bad, cudaStream_t st) {
@@ -188,13 +302,14 @@ cudaError_t launch_modularity(const void *off, bool off64, const uint32_t *tgt, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_lpa(const LpaArgs &a, int slots, int mode, bool off64, cudaStream_t st, int *grid_out) {
+cudaError_t launch_lpa(const LpaArgs &a, int slots, int mode, bool off64, cudaStream_t st, int *grid_out,
+                       bool batch) {
   switch (slots) {
-    case 1: return launch_lpa_slots<1>(a, mode, off64, st, grid_out);
-    case 2: return launch_lpa_slots<2>(a, mode, off64, st, grid_out);
-    case 4: return launch_lpa_slots<4>(a, mode, off64, st, grid_out);
-    case 8: return launch_lpa_slots<8>(a, mode, off64, st, grid_out);
-    case 16: return launch_lpa_slots<16>(a, mode, off64, st, grid_out);
+    case 1: return launch_lpa_slots<1>(a, mode, off64, batch, st, grid_out);
+    case 2: return launch_lpa_slots<2>(a, mode, off64, batch, st, grid_out);
+    case 4: return launch_lpa_slots<4>(a, mode, off64, batch, st, grid_out);
+    case 8: return launch_lpa_slots<8>(a, mode, off64, batch, st, grid_out);
+    case 16: return launch_lpa_slots<16>(a, mode, off64, batch, st, grid_out);
     default: return cudaErrorInvalidValue;
   }
 }

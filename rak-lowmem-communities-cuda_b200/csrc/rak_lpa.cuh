@@ -45,14 +45,15 @@ __device__ __forceinline__ float edge_w(const float *wt, int64_t e) {
 // during the launch.
 template <int S, bool UNIT>
 __device__ __forceinline__ void scan_range(Sketch<S> &sk, uint32_t u, int64_t e, int64_t ee, int st,
-                                           const uint32_t *tgt, const float *wt, const uint32_t *vin) {
+                                           const uint32_t *tgt, const float *wt, const uint32_t *vin,
+                                           uint32_t base) {
   constexpr int B = 4;
   uint32_t t[B];
   float w[B];
 #pragma unroll
   for (int j = 0; j < B; ++j) {
     const int64_t x = e + int64_t(j) * st;
-    t[j] = x < ee ? __ldg(tgt + x) : u;
+    t[j] = x < ee ? base + __ldg(tgt + x) : u;
     w[j] = x < ee ? edge_w<UNIT>(wt, x) : 0.0f;
   }
   while (e < ee) {
@@ -65,7 +66,7 @@ __device__ __forceinline__ void scan_range(Sketch<S> &sk, uint32_t u, int64_t e,
 #pragma unroll
     for (int j = 0; j < B; ++j) {
       const int64_t x = en + int64_t(j) * st;
-      t2[j] = x < ee ? __ldg(tgt + x) : u;
+      t2[j] = x < ee ? base + __ldg(tgt + x) : u;
       w2[j] = x < ee ? edge_w<UNIT>(wt, x) : 0.0f;
     }
 #pragma unroll
@@ -80,11 +81,12 @@ __device__ __forceinline__ void scan_range(Sketch<S> &sk, uint32_t u, int64_t e,
 // Exact weights of the sketch keys in edge order (inc/rakLowmem.hxx:154-162), one lane.
 template <int S, bool UNIT>
 __device__ __forceinline__ void rescan_range(Sketch<S> &sk, uint32_t u, int64_t e, int64_t ee,
-                                             const uint32_t *tgt, const float *wt, const uint32_t *vin) {
+                                             const uint32_t *tgt, const float *wt, const uint32_t *vin,
+                                             uint32_t base) {
 #pragma unroll
   for (int i = 0; i < S; ++i) sk.w[i] = 0.0f;
   for (; e < ee; ++e) {
-    const uint32_t v = __ldg(tgt + e);
+    const uint32_t v = base + __ldg(tgt + e);
     if (v == u) continue;
     const uint32_t c = vin[v];
     const float w = edge_w<UNIT>(wt, e);
@@ -97,17 +99,17 @@ __device__ __forceinline__ void rescan_range(Sketch<S> &sk, uint32_t u, int64_t 
 // Marks neighbours e, e+st, ... < ee of a moved vertex u as affected (inc/rakCuda.hxx:95-103),
 // except u itself (the reference CPU loop clears u after marking, inc/rakLowmem.hxx:203,209).
 __device__ __forceinline__ void mark_range(uint32_t u, int64_t e, int64_t ee, int st, const uint32_t *tgt,
-                                           uint8_t *fout) {
+                                           uint8_t *fout, uint32_t base) {
   for (; e + 3 * int64_t(st) < ee; e += 4 * int64_t(st)) {
-    const uint32_t v0 = __ldg(tgt + e), v1 = __ldg(tgt + e + st), v2 = __ldg(tgt + e + 2 * st),
-                   v3 = __ldg(tgt + e + 3 * st);
+    const uint32_t v0 = base + __ldg(tgt + e), v1 = base + __ldg(tgt + e + st),
+                   v2 = base + __ldg(tgt + e + 2 * st), v3 = base + __ldg(tgt + e + 3 * st);
     if (v0 != u) fout[v0] = 1;
     if (v1 != u) fout[v1] = 1;
     if (v2 != u) fout[v2] = 1;
     if (v3 != u) fout[v3] = 1;
   }
   for (; e < ee; e += st) {
-    const uint32_t v = __ldg(tgt + e);
+    const uint32_t v = base + __ldg(tgt + e);
     if (v != u) fout[v] = 1;
   }
 }
@@ -118,25 +120,25 @@ __device__ __forceinline__ void mark_range(uint32_t u, int64_t e, int64_t ee, in
 template <int S, bool UNIT>
 __device__ __forceinline__ void exact_group_scan(Sketch<S> &sk, uint32_t u, int64_t eb, int64_t ee, int G,
                                                  int g, int s, bool rescan, const uint32_t *tgt,
-                                                 const float *wt, const uint32_t *vin) {
+                                                 const float *wt, const uint32_t *vin, uint32_t base) {
   const unsigned gmask = G == 32 ? FULL : (((1u << G) - 1u) << (g * G));
   for (int pass = 0; pass < (rescan ? 2 : 1); ++pass) {
     if (pass == 1) {
 #pragma unroll
       for (int i = 0; i < S; ++i) sk.w[i] = 0.0f;
     }
-    for (int64_t base = eb; base < ee; base += G) {
-      const int64_t e = base + s;
+    for (int64_t e0 = eb; e0 < ee; e0 += G) {
+      const int64_t e = e0 + s;
       uint32_t c = NONE;
       float w = 0.0f;
       int ok = 0;
       if (e < ee) {
-        const uint32_t v = __ldg(tgt + e);
+        const uint32_t v = base + __ldg(tgt + e);
         w = edge_w<UNIT>(wt, e);
         c = vin[v];
         ok = v != u;
       }
-      const int cnt = int(ee - base < G ? ee - base : G);
+      const int cnt = int(ee - e0 < G ? ee - e0 : G);
       for (int t = 0; t < cnt; ++t) {
         const uint32_t ct = __shfl_sync(gmask, c, g * G + t);
         const float wt_ = __shfl_sync(gmask, w, g * G + t);
@@ -154,6 +156,26 @@ __device__ __forceinline__ void exact_group_scan(Sketch<S> &sk, uint32_t u, int6
   }
 }
 
+// Batches: a vertex's graph, whether that graph has converged, and its first vertex (the offset
+// of the graph's local target ids). Single graphs: never finished, offset 0.
+template <bool BATCH>
+__device__ __forceinline__ bool graph_of(const LpaArgs &a, uint32_t u, uint32_t &gi, uint32_t &base) {
+  if constexpr (BATCH) {
+    gi = __ldg(a.gid + u);
+    base = uint32_t(__ldg(a.vbase + gi));
+    return a.gdone[gi] != 0;
+  } else {
+    gi = 0;
+    base = 0;
+    return false;
+  }
+}
+
+template <bool BATCH>
+__device__ __forceinline__ void count_move(const LpaArgs &a, uint32_t gi, int it) {
+  if constexpr (BATCH) atomicAdd(a.gchanged + int64_t(it & 1) * a.ngraphs + gi, 1ull);
+}
+
 __device__ __forceinline__ bool move_rule(float w, uint32_t c, uint32_t d, bool pickless) {
   // inc/rakLowmem.hxx:203 (w>0 && c!=d) and inc/rakLowmemCuda.hxx:309 (pickless: no larger label)
   return w > 0.0f && c != d && !(pickless && c > d);
@@ -162,7 +184,7 @@ __device__ __forceinline__ bool move_rule(float w, uint32_t c, uint32_t d, bool 
 // Region 6: one lane per vertex. Items are collected into a per-warp queue of active vertices
 // (inactive ones are settled at once), and the queue is processed 32 vertices at a time so every
 // lane has work; region 6 is sorted by degree, so a batch holds vertices of similar degree.
-template <int S, int MODE, class O, bool UNIT>
+template <int S, int MODE, class O, bool UNIT, bool BATCH>
 __device__ __forceinline__ int lane_collect(const LpaArgs &a, const Regions &rg, int64_t local, const uint32_t *vin,
                                             uint32_t *vout, const uint8_t *fin, uint32_t *q, int qn) {
   const int lane = threadIdx.x & 31;
@@ -171,7 +193,8 @@ __device__ __forceinline__ int lane_collect(const LpaArgs &a, const Regions &rg,
   uint32_t u = 0;
   if (idx < rg.vcount[REG_LANE]) {
     u = __ldg(a.order + rg.vbegin[REG_LANE] + idx);
-    act = fin[u] != 0;
+    uint32_t gi, base;
+    act = fin[u] != 0 && !graph_of<BATCH>(a, u, gi, base);
     if constexpr (MODE != MODE_ASYNC)
       if (!act) vout[u] = vin[u];
   }
@@ -181,20 +204,22 @@ __device__ __forceinline__ int lane_collect(const LpaArgs &a, const Regions &rg,
   return qn + __popc(m);
 }
 
-template <int S, int MODE, class O, bool UNIT>
+template <int S, int MODE, class O, bool UNIT, bool BATCH>
 __device__ __forceinline__ void lane_batch(const LpaArgs &a, const G_<O> &g, const uint32_t *q, int count,
-                                           bool pickless, const uint32_t *vin, uint32_t *vout, uint8_t *fin,
-                                           uint8_t *fout, Counters &cnt) {
+                                           int it, bool pickless, const uint32_t *vin, uint32_t *vout,
+                                           uint8_t *fin, uint8_t *fout, Counters &cnt) {
   const int lane = threadIdx.x & 31;
   if (lane >= count) return;
   const uint32_t u = q[lane];
   const uint32_t d = vin[u];
+  uint32_t gi, base;
+  graph_of<BATCH>(a, u, gi, base);
   const int64_t eb = int64_t(__ldg(g.off + u)), ee = int64_t(__ldg(g.off + u + 1));
   Sketch<S> sk;
   sk_clear(sk);
-  scan_range<S, UNIT>(sk, u, eb, ee, 1, g.tgt, g.wt, vin);
+  scan_range<S, UNIT>(sk, u, eb, ee, 1, g.tgt, g.wt, vin, base);
   if constexpr (MODE == MODE_SYNC && S > 1)
-    if (a.rescan) rescan_range<S, UNIT>(sk, u, eb, ee, g.tgt, g.wt, vin);
+    if (a.rescan) rescan_range<S, UNIT>(sk, u, eb, ee, g.tgt, g.wt, vin, base);
   uint32_t c;
   float w;
   sk_choose(sk, c, w);
@@ -210,34 +235,35 @@ __device__ __forceinline__ void lane_batch(const LpaArgs &a, const G_<O> &g, con
   if (moved) {
     cnt.changed += 1;
     cnt.moved_edges += (unsigned long long)(ee - eb);
-    mark_range(u, eb, ee, 1, g.tgt, fout);
+    count_move<BATCH>(a, gi, it);
+    mark_range(u, eb, ee, 1, g.tgt, fout, base);
   }
 }
 
 // Regions 1..5: aligned groups of G lanes per vertex.
-template <int S, int MODE, class O, bool UNIT>
-__device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, const G_<O> &g, int r, int64_t local, bool pickless,
-                                           const uint32_t *vin, uint32_t *vout, uint8_t *fin, uint8_t *fout,
-                                           Counters &cnt) {
+template <int S, int MODE, class O, bool UNIT, bool BATCH>
+__device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, const G_<O> &g, int r, int64_t local,
+                                           int it, bool pickless, const uint32_t *vin, uint32_t *vout,
+                                           uint8_t *fin, uint8_t *fout, Counters &cnt) {
   const int G = region_group(r);
   const int lane = threadIdx.x & 31, grp = lane / G, s = lane & (G - 1);
   const int64_t idx = local * (32 / G) + grp;
   const bool valid = idx < rg.vcount[r];
-  uint32_t u = 0, d = 0;
+  uint32_t u = 0, d = 0, gi = 0, base = 0;
   int64_t eb = 0, ee = 0;
   bool active = false;
   if (valid) {
     u = __ldg(a.order + rg.vbegin[r] + idx);
     d = vin[u];
-    active = fin[u] != 0;
+    active = fin[u] != 0 && !graph_of<BATCH>(a, u, gi, base);
     if (active) { eb = int64_t(__ldg(g.off + u)); ee = int64_t(__ldg(g.off + u + 1)); }
   }
   Sketch<S> sk;
   sk_clear(sk);
   if constexpr (MODE == MODE_SYNC) {
-    if (active) exact_group_scan<S, UNIT>(sk, u, eb, ee, G, grp, s, S > 1 && a.rescan, g.tgt, g.wt, vin);
+    if (active) exact_group_scan<S, UNIT>(sk, u, eb, ee, G, grp, s, S > 1 && a.rescan, g.tgt, g.wt, vin, base);
   } else {
-    if (active) scan_range<S, UNIT>(sk, u, eb + s, ee, G, g.tgt, g.wt, vin);
+    if (active) scan_range<S, UNIT>(sk, u, eb + s, ee, G, g.tgt, g.wt, vin, base);
     sk_tree(sk, G);
   }
   uint32_t c;
@@ -253,9 +279,9 @@ __device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, 
     } else {
       vout[u] = moved ? c : d;
     }
-    if (moved) { cnt.changed += 1; cnt.moved_edges += (unsigned long long)(ee - eb); }
+    if (moved) { cnt.changed += 1; cnt.moved_edges += (unsigned long long)(ee - eb); count_move<BATCH>(a, gi, it); }
   }
-  if (moved) mark_range(u, eb + s, ee, G, g.tgt, fout);
+  if (moved) mark_range(u, eb + s, ee, G, g.tgt, fout, base);
 }
 
 // Region 0: one chunk of a split vertex per item. In the synchronous exact mode chunk 0's warp
@@ -263,7 +289,7 @@ __device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, 
 // warp builds a partial sketch (lane-strided, tree-merged), stores it, and the last chunk to
 // arrive merges all partial sketches in a fixed order and makes the move; its neighbours are
 // marked in a second phase after the iteration's barrier.
-template <int S, int MODE, class O, bool UNIT>
+template <int S, int MODE, class O, bool UNIT, bool BATCH>
 __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, const G_<O> &g, int64_t local, int it, bool pickless,
                                          const uint32_t *vin, uint32_t *vout, uint8_t *fin, uint8_t *fout,
                                          Counters &cnt) {
@@ -272,13 +298,15 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
   const int64_t first = __ldg(a.hub_first + h), nch = __ldg(a.hub_first + h + 1) - first, j = local - first;
   const uint32_t u = __ldg(a.order + rg.vbegin[REG_HUB] + h);
   const int64_t eb = int64_t(__ldg(g.off + u)), ee = int64_t(__ldg(g.off + u + 1));
+  uint32_t gi, base;
+  const bool gfin = graph_of<BATCH>(a, u, gi, base);  // stable within an iteration
   if constexpr (MODE == MODE_SYNC) {
     if (j != 0) return;
     const uint32_t d = vin[u];
-    const bool active = fin[u] != 0;
+    const bool active = fin[u] != 0 && !gfin;
     Sketch<S> sk;
     sk_clear(sk);
-    if (active) exact_group_scan<S, UNIT>(sk, u, eb, ee, 32, 0, lane, S > 1 && a.rescan, g.tgt, g.wt, vin);
+    if (active) exact_group_scan<S, UNIT>(sk, u, eb, ee, 32, 0, lane, S > 1 && a.rescan, g.tgt, g.wt, vin, base);
     uint32_t c;
     float w;
     sk_choose(sk, c, w);
@@ -286,13 +314,15 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
     if (lane == 0) {
       vout[u] = moved ? c : d;
       if (active) { cnt.processed += 1; cnt.edges += (unsigned long long)(ee - eb); }
-      if (moved) { cnt.changed += 1; cnt.moved_edges += (unsigned long long)(ee - eb); }
+      if (moved) { cnt.changed += 1; cnt.moved_edges += (unsigned long long)(ee - eb); count_move<BATCH>(a, gi, it); }
     }
-    if (moved) mark_range(u, eb + lane, ee, 32, g.tgt, fout);
+    if (moved) mark_range(u, eb + lane, ee, 32, g.tgt, fout, base);
     return;
   } else {
     bool active;
-    if constexpr (MODE == MODE_SPLIT) {
+    if (gfin) {
+      active = false;
+    } else if constexpr (MODE == MODE_SPLIT) {
       active = fin[u] != 0;
     } else {
       // All chunks of u agree on whether u is processed this iteration: the first chunk to get
@@ -318,7 +348,7 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
     Sketch<S> sk;
     sk_clear(sk);
     const int64_t cb = eb + j * a.hub_chunk, ce = cb + a.hub_chunk < ee ? cb + a.hub_chunk : ee;
-    if (active) scan_range<S, UNIT>(sk, u, cb + lane, ce, 32, g.tgt, g.wt, vin);
+    if (active) scan_range<S, UNIT>(sk, u, cb + lane, ce, 32, g.tgt, g.wt, vin, base);
     sk_tree(sk, 32);
     unsigned int last = 0;
     if (lane == 0) {
@@ -369,6 +399,7 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
       if (moved) {
         cnt.changed += 1;
         cnt.moved_edges += (unsigned long long)(ee - eb);
+        count_move<BATCH>(a, gi, it);
         a.hub_moved[h] = it;
         atomicAdd(a.stats + STATS_STRIDE * it + STAT_HUBS_MOVED, 1ull);
       }
@@ -376,7 +407,7 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
   }
 }
 
-template <int S, int MODE, class O, bool UNIT>
+template <int S, int MODE, class O, bool UNIT, bool BATCH>
 __global__ void __launch_bounds__(256, 3) lpa_run(const LpaArgs a) {
   const G_<O> g{static_cast<const O *>(a.off), a.tgt, a.wt};
   RunState *rs = static_cast<RunState *>(a.rs);
@@ -412,21 +443,21 @@ __global__ void __launch_bounds__(256, 3) lpa_run(const LpaArgs a) {
       while (item >= rg.ibegin[r + 1]) ++r;
       const int64_t local = item - rg.ibegin[r];
       if (r == REG_LANE) {
-        qn = lane_collect<S, MODE, O, UNIT>(a, rg, local, vin, vout, fin, q, qn);
+        qn = lane_collect<S, MODE, O, UNIT, BATCH>(a, rg, local, vin, vout, fin, q, qn);
         if (qn >= 32) {
-          lane_batch<S, MODE, O, UNIT>(a, g, q, 32, pickless, vin, vout, fin, fout, cnt);
+          lane_batch<S, MODE, O, UNIT, BATCH>(a, g, q, 32, it, pickless, vin, vout, fin, fout, cnt);
           __syncwarp();
           if (lane < qn - 32) q[lane] = q[32 + lane];
           __syncwarp();
           qn -= 32;
         }
       } else if (r == REG_HUB) {
-        hub_item<S, MODE, O, UNIT>(a, rg, g, local, it, pickless, vin, vout, fin, fout, cnt);
+        hub_item<S, MODE, O, UNIT, BATCH>(a, rg, g, local, it, pickless, vin, vout, fin, fout, cnt);
       } else {
-        group_item<S, MODE, O, UNIT>(a, rg, g, r, local, pickless, vin, vout, fin, fout, cnt);
+        group_item<S, MODE, O, UNIT, BATCH>(a, rg, g, r, local, it, pickless, vin, vout, fin, fout, cnt);
       }
     }
-    if (qn > 0) lane_batch<S, MODE, O, UNIT>(a, g, q, qn, pickless, vin, vout, fin, fout, cnt);
+    if (qn > 0) lane_batch<S, MODE, O, UNIT, BATCH>(a, g, q, qn, it, pickless, vin, vout, fin, fout, cnt);
     __syncwarp();
     const unsigned long long ch = warp_sum((unsigned long long)cnt.changed);
     const unsigned long long ed = warp_sum(cnt.edges);
@@ -446,7 +477,8 @@ __global__ void __launch_bounds__(256, 3) lpa_run(const LpaArgs a) {
     if (!grid_barrier(rs, ++epoch, a.timeout_ns)) return;
     const unsigned long long changed = __ldcg(a.stats + STATS_STRIDE * it + STAT_CHANGED);
     const bool test = !pickless || a.check_on_pickless;
-    const bool done = it + 1 >= a.iters || (test && double(changed) / double(a.n) <= a.tolerance);
+    // Batches finish when no graph is still running (decided in the per-graph phase below).
+    const bool done = !BATCH && (it + 1 >= a.iters || (test && double(changed) / double(a.n) <= a.tolerance));
     // The synchronous split mode completes the next flags even on the last iteration, so a
     // single step returns them whole.
     if (MODE != MODE_SYNC && (!done || MODE == MODE_SPLIT) && a.nchunks > 0 && __ldcg(a.stats + STATS_STRIDE * it + STAT_HUBS_MOVED) > 0) {
@@ -458,8 +490,43 @@ __global__ void __launch_bounds__(256, 3) lpa_run(const LpaArgs a) {
         const int64_t eb = int64_t(__ldg(g.off + u)), ee = int64_t(__ldg(g.off + u + 1));
         const int64_t j = i - __ldg(a.hub_first + h);
         const int64_t cb = eb + j * a.hub_chunk, ce = cb + a.hub_chunk < ee ? cb + a.hub_chunk : ee;
-        mark_range(u, cb + lane, ce, 32, g.tgt, fout);
+        uint32_t gi, base;
+        graph_of<BATCH>(a, u, gi, base);
+        mark_range(u, cb + lane, ce, 32, g.tgt, fout, base);
       }
+    }
+    if constexpr (BATCH) {
+      // Per-graph convergence, each graph by one thread: the rule of the single-graph loop applied
+      // to the graph's own changed count and vertex count; also clears the graph's counter for the
+      // iteration after next.
+      const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+      unsigned int run = 0;
+      for (int64_t gi = tid; gi < a.ngraphs; gi += nt) {
+        if (a.gdone[gi]) continue;
+        const int64_t ng = a.vbase[gi + 1] - a.vbase[gi];
+        const unsigned long long c = __ldcg(a.gchanged + int64_t(it & 1) * a.ngraphs + gi);
+        if (ng == 0 || it + 1 >= a.iters || (test && double(c) / double(ng) <= a.tolerance)) {
+          a.gdone[gi] = 1;
+          a.giters[gi] = it + 1;
+        } else {
+          ++run;
+        }
+        a.gchanged[int64_t((it + 1) & 1) * a.ngraphs + gi] = 0ull;
+      }
+      run = warp_sum(run);
+      if (lane == 0 && run) atomicAdd(a.running + it, run);
+      if constexpr (MODE != MODE_ASYNC) {
+        uint4 *f4 = reinterpret_cast<uint4 *>(fin);
+        const int64_t n16 = a.n >> 4;
+        for (int64_t i = tid; i < n16; i += nt) f4[i] = make_uint4(0, 0, 0, 0);
+        for (int64_t i = (n16 << 4) + tid; i < a.n; i += nt) fin[i] = 0;
+      }
+      if (!grid_barrier(rs, ++epoch, a.timeout_ns)) return;
+      if (__ldcg(a.running + it) == 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) rs->iterations = unsigned(it + 1);
+        return;
+      }
+      continue;
     }
     if (done) {
       if (blockIdx.x == 0 && threadIdx.x == 0) rs->iterations = unsigned(it + 1);
@@ -478,17 +545,18 @@ __global__ void __launch_bounds__(256, 3) lpa_run(const LpaArgs a) {
 }
 
 template <int S>
-cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, cudaStream_t st, int *grid_out) {
+cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, bool batch, cudaStream_t st, int *grid_out) {
   const void *fn = nullptr;
   const bool unit = a.wt == nullptr;
-#define RAK_PICK(M, O, U) \
-  if (mode == M && off64 == (sizeof(O) == 8) && unit == U) fn = reinterpret_cast<const void *>(&lpa_run<S, M, O, U>);
-  RAK_PICK(MODE_ASYNC, int32_t, false) RAK_PICK(MODE_ASYNC, int32_t, true)
-  RAK_PICK(MODE_ASYNC, int64_t, false) RAK_PICK(MODE_ASYNC, int64_t, true)
-  RAK_PICK(MODE_SYNC, int32_t, false) RAK_PICK(MODE_SYNC, int32_t, true)
-  RAK_PICK(MODE_SYNC, int64_t, false) RAK_PICK(MODE_SYNC, int64_t, true)
-  RAK_PICK(MODE_SPLIT, int32_t, false) RAK_PICK(MODE_SPLIT, int32_t, true)
-  RAK_PICK(MODE_SPLIT, int64_t, false) RAK_PICK(MODE_SPLIT, int64_t, true)
+#define RAK_PICK(M, O, U, B)                                                          \
+  if (mode == M && off64 == (sizeof(O) == 8) && unit == U && batch == B)             \
+    fn = reinterpret_cast<const void *>(&lpa_run<S, M, O, U, B>);
+#define RAK_PICK_MODE(M)                                                             \
+  RAK_PICK(M, int32_t, false, false) RAK_PICK(M, int32_t, true, false)                \
+  RAK_PICK(M, int64_t, false, false) RAK_PICK(M, int64_t, true, false)                \
+  RAK_PICK(M, int64_t, false, true) RAK_PICK(M, int64_t, true, true)
+  RAK_PICK_MODE(MODE_ASYNC) RAK_PICK_MODE(MODE_SYNC) RAK_PICK_MODE(MODE_SPLIT)
+#undef RAK_PICK_MODE
 #undef RAK_PICK
   if (!fn) return cudaErrorInvalidValue;
   int dev = 0, sms = 0, per_sm = 0;
@@ -503,8 +571,19 @@ cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, cudaStream_
   if (want < grid) grid = want;
   if (grid < 1) grid = 1;
   if (grid_out) *grid_out = int(grid);
+  // Cooperative attribute through cudaLaunchKernelEx: co-residency is guaranteed (the grid
+  // barrier relies on it) and the launch can be captured into a CUDA graph.
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(grid));
+  cfg.blockDim = dim3(256);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
   void *args[] = {const_cast<LpaArgs *>(&a)};
-  return cudaLaunchCooperativeKernel(fn, dim3(unsigned(grid)), dim3(256), args, 0, st);
+  return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
 }  // namespace rak

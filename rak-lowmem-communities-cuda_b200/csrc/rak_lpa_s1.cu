@@ -2,5 +2,5 @@
 #include "rak_lpa.cuh"
 
 namespace rak {
-template cudaError_t launch_lpa_slots<1>(const LpaArgs &, int, bool, cudaStream_t, int *);
+template cudaError_t launch_lpa_slots<1>(const LpaArgs &, int, bool, bool, cudaStream_t, int *);
 }

@@ -55,6 +55,12 @@ class rak_result(C.Structure):
                 ("loop_ms", C.c_float), ("reserved_f", C.c_float), ("modularity", C.c_double)]
 
 
+class rak_batch_csr(C.Structure):
+    _fields_ = [("graphs", C.c_int64), ("n", C.c_int64), ("m", C.c_int64), ("location", C.c_int32),
+                ("reserved", C.c_int32), ("graph_offsets", C.c_void_p), ("offsets", C.c_void_p),
+                ("targets", C.c_void_p), ("weights", C.c_void_p)]
+
+
 class rak_host_csr(C.Structure):
     _fields_ = [("n", C.c_int64), ("m", C.c_int64), ("offsets", C.c_void_p), ("targets", C.c_void_p),
                 ("weights", C.c_void_p), ("truth", C.c_void_p)]
@@ -82,6 +88,13 @@ _sig("rak_graph_device_bytes", C.c_uint64, P)
 _sig("rak_graph_run", C.c_int, P, P, P, C.POINTER(rak_options), P, C.POINTER(rak_result))
 _sig("rak_graph_step", C.c_int, P, P, C.POINTER(rak_options), C.c_int, P, P, P, P, C.POINTER(C.c_uint64))
 _sig("rak_modularity_f64", C.c_int, P, C.POINTER(rak_csr), P, C.POINTER(C.c_double))
+_sig("rak_batch_create", C.c_int, P, C.POINTER(rak_batch_csr), C.POINTER(rak_options), C.POINTER(P))
+_sig("rak_batch_destroy", C.c_int, P)
+_sig("rak_batch_launch", C.c_int, P, P, P, C.POINTER(rak_options), P)
+_sig("rak_batch_results", C.c_int, P, P, P, C.POINTER(rak_result))
+_sig("rak_batch_capture", C.c_int, P, P, P, C.POINTER(rak_options), P)
+_sig("rak_batch_replay", C.c_int, P, P)
+_sig("rak_batch_modularity_f64", C.c_int, P, P, P, P)
 _sig("rak_lowmem_cuda_noalloc", C.c_int, C.c_int, P, C.POINTER(rak_csr), P, C.POINTER(rak_options), P,
      C.POINTER(rak_result))
 NOALLOC_SCRATCH_BYTES = 64 << 20
@@ -173,22 +186,33 @@ class _Owned:
         self.h = h
 
     def __del__(self):
-        _lib.rak_host_csr_free(C.byref(self.h))
+        if _lib is not None:
+            _lib.rak_host_csr_free(C.byref(self.h))
+
+
+class _View:
+    """Array interface over library-owned memory that keeps the owner alive: every numpy array
+    (and slice) made from it references this object, so the memory outlives all of them."""
+
+    def __init__(self, ptr, count, dtype, owner):
+        self.__array_interface__ = {"data": (ptr, False), "shape": (count,), "typestr": np.dtype(dtype).str,
+                                    "version": 3}
+        self._owner = owner
 
 
 def _wrap_host(h: rak_host_csr) -> HostGraph:
     owner = _Owned(h)
     n, m = h.n, h.m
 
-    def arr(ptr, ctype, count, dtype):
+    def arr(ptr, count, dtype):
         if not ptr or count == 0:
             return np.zeros(count, dtype=dtype)
-        return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), shape=(count,)).view(dtype)
+        return np.asarray(_View(ptr, count, dtype, owner))
 
-    off = arr(h.offsets, C.c_int64, n + 1, np.int64)
-    tgt = arr(h.targets, C.c_uint32, m, np.uint32)
-    wt = arr(h.weights, C.c_float, m, np.float32) if h.weights else None
-    truth = arr(h.truth, C.c_uint32, n, np.uint32) if h.truth else None
+    off = arr(h.offsets, n + 1, np.int64)
+    tgt = arr(h.targets, m, np.uint32)
+    wt = arr(h.weights, m, np.float32) if h.weights else None
+    truth = arr(h.truth, n, np.uint32) if h.truth else None
     return HostGraph(off, tgt, wt, truth, owner)
 
 
@@ -250,7 +274,7 @@ class Context:
         _check(_lib.rak_ctx_create(device, C.byref(self._c)))
 
     def close(self):
-        if self._c:
+        if self._c and _lib is not None:
             _lib.rak_ctx_destroy(self._c)
             self._c = P()
 
@@ -337,7 +361,7 @@ class ResidentGraph:
         _check(_lib.rak_graph_create(ctx.handle, C.byref(c), C.byref(o), C.byref(self._g)), ctx.handle)
 
     def close(self):
-        if self._g:
+        if self._g and _lib is not None:
             _lib.rak_graph_destroy(self._g)
             self._g = P()
 
@@ -361,6 +385,97 @@ class ResidentGraph:
                                    aff_prev.data_ptr(), vcom_next.data_ptr(), aff_next.data_ptr(),
                                    C.byref(ch)), self.ctx.handle)
         return ch.value
+
+
+class HostBatch:
+    """Graphs concatenated into one CSR: graph g owns vertices [graph_offsets[g], graph_offsets[g+1]),
+    offsets (int64) index the concatenated targets (ids local to each graph) and weights."""
+
+    def __init__(self, graph_offsets, offsets, targets, weights=None, truths=None):
+        self.graph_offsets = np.ascontiguousarray(graph_offsets, dtype=np.int64)
+        self.offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        self.targets = np.ascontiguousarray(targets, dtype=np.uint32)
+        self.weights = None if weights is None else np.ascontiguousarray(weights, dtype=np.float32)
+        self.truths = truths
+        self.graphs = len(self.graph_offsets) - 1
+        self.n = int(self.graph_offsets[-1])
+        self.m = int(self.offsets[-1])
+
+    @staticmethod
+    def concat(graphs, weighted=None) -> "HostBatch":
+        """Packs HostGraphs into a batch (weights kept if every graph has them, unless weighted=False)."""
+        if weighted is None:
+            weighted = all(g.weights is not None for g in graphs) and len(graphs) > 0
+        go = np.zeros(len(graphs) + 1, np.int64)
+        go[1:] = np.cumsum([g.n for g in graphs])
+        eo = np.zeros(len(graphs) + 1, np.int64)
+        eo[1:] = np.cumsum([g.m for g in graphs])
+        off = np.empty(int(go[-1]) + 1, np.int64)
+        off[-1] = eo[-1]
+        for i, g in enumerate(graphs):
+            off[go[i]:go[i + 1]] = g.offsets[:-1].astype(np.int64) + eo[i]
+        tgt = np.concatenate([g.targets for g in graphs]) if graphs else np.zeros(0, np.uint32)
+        wt = np.concatenate([g.weights for g in graphs]) if weighted else None
+        truths = [g.truth for g in graphs] if all(g.truth is not None for g in graphs) and graphs else None
+        return HostBatch(go, off, tgt, wt, truths)
+
+    def graph(self, i) -> HostGraph:
+        a, b = int(self.graph_offsets[i]), int(self.graph_offsets[i + 1])
+        e0, e1 = int(self.offsets[a]), int(self.offsets[b])
+        return HostGraph(self.offsets[a:b + 1] - e0, self.targets[e0:e1],
+                         None if self.weights is None else self.weights[e0:e1])
+
+    def csr(self) -> rak_batch_csr:
+        return rak_batch_csr(self.graphs, self.n, self.m, HOST, 0, self.graph_offsets.ctypes.data,
+                             self.offsets.ctypes.data, self.targets.ctypes.data if self.m else None,
+                             self.weights.ctypes.data if self.weights is not None else None)
+
+
+class Batch:
+    """A device-resident batch of graphs (rak_batch): one persistent launch runs them all."""
+
+    def __init__(self, ctx: Context, host_batch: HostBatch, **opts):
+        self.ctx = ctx
+        self.graphs = host_batch.graphs
+        self.n = host_batch.n
+        self._b = P()
+        c = host_batch.csr()
+        o = options(**opts)
+        _check(_lib.rak_batch_create(ctx.handle, C.byref(c), C.byref(o), C.byref(self._b)), ctx.handle)
+
+    def close(self):
+        if self._b and _lib is not None:
+            _lib.rak_batch_destroy(self._b)
+            self._b = P()
+
+    def __del__(self):
+        self.close()
+
+    def launch(self, membership, q=None, **opts):
+        o = options(**opts)
+        _check(_lib.rak_batch_launch(self.ctx.handle, self._b, _ptr(q), C.byref(o), membership.data_ptr()),
+               self.ctx.handle)
+
+    def results(self):
+        it = np.zeros(self.graphs, np.int32)
+        r = rak_result()
+        _check(_lib.rak_batch_results(self.ctx.handle, self._b, it.ctypes.data if self.graphs else None,
+                                      C.byref(r)), self.ctx.handle)
+        return it, Result.of(r)
+
+    def capture(self, membership, q=None, **opts):
+        o = options(**opts)
+        _check(_lib.rak_batch_capture(self.ctx.handle, self._b, _ptr(q), C.byref(o), membership.data_ptr()),
+               self.ctx.handle)
+
+    def replay(self):
+        _check(_lib.rak_batch_replay(self.ctx.handle, self._b), self.ctx.handle)
+
+    def modularity(self, membership) -> np.ndarray:
+        q = np.zeros(max(self.graphs, 1), np.float64)
+        _check(_lib.rak_batch_modularity_f64(self.ctx.handle, self._b, membership.data_ptr(), q.ctypes.data),
+               self.ctx.handle)
+        return q[:self.graphs]
 
 
 def write_rakcsr(path: str, g: HostGraph):

@@ -28,7 +28,11 @@ int main() {
   try {
     auto a = rak_b200::rakLowmemStaticCuda<8>(x, {1});
     auto b = rak_b200::rakLowmemStaticCuda<1>(x, {1, 0.05, 20});
-    for (auto *r : {&a.membership, &b.membership}) {
+    rak_options sync;
+    rak_options_default(&sync);
+    sync.mode = RAK_MODE_SYNC;  // deterministic: checked against the oracle by the test
+    auto c = rak_b200::rakLowmemCuda<ToyGraph, uint32_t>(x, nullptr, {1}, 8, &sync);
+    for (auto *r : {&a.membership, &b.membership, &c.membership}) {
       for (size_t u = 0; u < r->size(); ++u) printf("%u ", unsigned((*r)[u]));
       printf("\n");
     }
