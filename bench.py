@@ -210,6 +210,117 @@ def cpu_baseline(g, budget_s=20.0):
                       f"on the same graph, best of {len(times)}"}
 
 
+def nmi(a, b):
+    """Normalised mutual information (arithmetic mean normalisation) of two labellings."""
+    a = np.unique(np.asarray(a), return_inverse=True)[1]
+    b = np.unique(np.asarray(b), return_inverse=True)[1]
+    n = len(a)
+    if n == 0:
+        return 1.0
+    ka, kb = a.max() + 1, b.max() + 1
+    joint = np.bincount(a.astype(np.int64) * kb + b, minlength=ka * kb).astype(np.float64)
+    joint = joint[joint > 0] / n
+    pa = np.bincount(a) / n
+    pb = np.bincount(b) / n
+    ha = -np.sum(pa[pa > 0] * np.log(pa[pa > 0]))
+    hb = -np.sum(pb[pb > 0] * np.log(pb[pb > 0]))
+    hab = -np.sum(joint * np.log(joint))
+    mi = ha + hb - hab
+    return 1.0 if ha + hb == 0 else 2.0 * mi / (ha + hb)
+
+
+def batch_mix(count, seed, threads):
+    """The batched-launch mix: vertex counts log-uniform in 2^10..2^18; half symmetric R-MAT
+    (edge factor uniform in 8..32, power-of-two sizes), half planted-partition SBM (k uniform in
+    8..1024 equal blocks, clamped to n, average degree 16, p_in/p_out = 20); unit weights."""
+    import rak_lowmem as rl
+    rng = np.random.default_rng(seed)
+    graphs = []
+    for i in range(count):
+        if i % 2 == 0:
+            scale = int(rng.integers(10, 19))
+            graphs.append(rl.gen_rmat(scale, float(rng.integers(8, 33)), seed=seed * 100003 + i, threads=threads))
+        else:
+            n = int(round(2.0 ** rng.uniform(10, 18)))
+            k = min(int(rng.integers(8, 1025)), n)
+            graphs.append(rl.gen_sbm(n, k, 16.0, 20.0, seed=seed * 100003 + i, threads=threads))
+    return graphs
+
+
+def batched_leg(ctx, count, steps, threads, stream):
+    """Batched persistent launch (captured in a CUDA graph) vs a loop of plain per-graph runs on
+    resident graphs, same mix, same options; both timed on the device with CUDA events."""
+    import torch
+    import rak_lowmem as rl
+    t0 = time.time()
+    graphs = batch_mix(count, 4, threads)
+    hb = rl.HostBatch.concat(graphs, weighted=False)
+    log(f"[batched] {count} graphs, {hb.n} vertices, {hb.m} edges generated in {time.time() - t0:.1f}s")
+    b = rl.Batch(ctx, hb)
+    out = torch.empty(hb.n, dtype=torch.int32, device="cuda")
+    b.capture(out)
+    for _ in range(2):
+        b.replay()
+        b.results()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        b.replay()
+    e1.record(stream)
+    iters, tot = b.results()
+    t_batch = e0.elapsed_time(e1) / 1e3 / steps
+    lab = out.cpu().numpy().view(np.uint32)
+    q_batch = b.modularity(out)
+    # the loop: one resident graph per member (device views into the same arrays), one plain
+    # rak_graph_run per graph
+    off_d = torch.from_numpy(hb.offsets).cuda()
+    tgt_d = torch.from_numpy(hb.targets.view(np.int32)).cuda()
+    members, loop_out = [], []
+    for i in range(count):
+        a, z = int(hb.graph_offsets[i]), int(hb.graph_offsets[i + 1])
+        e_a = int(hb.offsets[a])
+        off_i = (off_d[a:z + 1] - e_a).contiguous()
+        csr = rl.rak_csr(z - a, int(hb.offsets[z]) - e_a, 64, rl.DEVICE, off_i.data_ptr(),
+                         tgt_d.data_ptr() + 4 * e_a if z > a else None, None)
+        members.append((off_i, rl.ResidentGraph(ctx, csr, validate=0)))
+    loop_lab = torch.empty_like(out)
+    for i, (_, rg) in enumerate(members):   # warm-up: one run of every member
+        a, z = int(hb.graph_offsets[i]), int(hb.graph_offsets[i + 1])
+        if z > a:
+            rg.run(loop_lab[a:z])
+    e0.record(stream)
+    for _ in range(steps):
+        for i, (_, rg) in enumerate(members):
+            a, z = int(hb.graph_offsets[i]), int(hb.graph_offsets[i + 1])
+            if z > a:
+                rg.run(loop_lab[a:z])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_loop = e0.elapsed_time(e1) / 1e3 / steps
+    q_loop = b.modularity(loop_lab)
+    loop_np = loop_lab.cpu().numpy().view(np.uint32)
+    nmis, nmis_loop = [], []
+    for i, g in enumerate(graphs):
+        if g.truth is not None:
+            a, z = int(hb.graph_offsets[i]), int(hb.graph_offsets[i + 1])
+            nmis.append(nmi(lab[a:z], g.truth))
+            nmis_loop.append(nmi(loop_np[a:z], g.truth))
+    for _, rg in members:
+        rg.close()
+    b.close()
+    return {"graphs": count, "vertices": int(hb.n), "edges": int(hb.m),
+            "mix": "half symmetric R-MAT (ef U{8..32}, n = 2^U{10..18}), half planted SBM (k U{8..1024}, "
+                   "avg degree 16, p_in/p_out 20, n log-uniform 2^10..2^18), unit weights, seed 4",
+            "graphs_per_s": count / t_batch, "ms_per_batch": 1e3 * t_batch,
+            "loop_graphs_per_s": count / t_loop, "loop_ms": 1e3 * t_loop, "speedup": t_loop / t_batch,
+            "batched_path": "rak_batch_capture + rak_batch_replay (one persistent launch in a CUDA graph)",
+            "loop_path": "rak_graph_run per resident graph (one persistent launch + read-back each)",
+            "edges_per_s": tot.traversed_edges / t_batch, "iterations_max": int(iters.max()),
+            "modularity_mean": float(np.mean(q_batch)), "loop_modularity_mean": float(np.mean(q_loop)),
+            "nmi_sbm_mean": float(np.mean(nmis)) if nmis else None,
+            "loop_nmi_sbm_mean": float(np.mean(nmis_loop)) if nmis_loop else None}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -220,6 +331,8 @@ def main():
     ap.add_argument("--slots", type=int, default=8)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-graphs", type=int, default=256,
+                    help="graphs in the batched-launch comparison (4096 = the full mix; 0 = skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -349,6 +462,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(g)
+    batched = None
+    if args.batch_graphs > 0:
+        batched = batched_leg(ctx, args.batch_graphs, 3, threads, stream)
 
     if rank == 0:
         last = results[-1]
@@ -360,7 +476,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
-                "gpu_launches": 3 * args.steps,
+                "gpu_launches": 3 * args.steps, "batched": batched,
                 "run": {"iterations": last.iterations, "traversed_edges_per_step": last.traversed_edges,
                         "processed_vertices_per_step": last.processed_vertices,
                         "moved_vertices_per_step": last.moved_vertices, "loop_ms": last.loop_ms,

@@ -204,6 +204,47 @@ rak_status rak_batch_replay(rak_ctx *ctx, rak_batch *b);
 /* FP64 modularity of every graph (membership: device, local labels); q: host, `graphs` entries. */
 rak_status rak_batch_modularity_f64(rak_ctx *ctx, rak_batch *b, const uint32_t *membership, double *q);
 
+/* ---- serving: continuous batching of requests --------------------------------------------- */
+/* A request loop (its own host thread) that keeps admitted graphs resident on the device, admits
+ * waiting requests as soon as device-memory budget and a launch slot are free, packs them into a
+ * batch and runs it as one persistent launch; several launches run at once on separate streams
+ * (each capped to its share of the SMs), so requests that arrive while others are on the GPU
+ * overlap with them. No reference counterpart (the reference runs one graph per call). */
+typedef struct rak_server rak_server;
+
+typedef struct rak_server_options {
+  uint64_t budget_bytes;        /* device bytes for admitted requests (graphs + working buffers) */
+  int32_t max_graphs_per_launch;/* requests packed into one launch at most [256] */
+  int32_t slots;                /* launches in flight at once, each on its own stream [2] */
+  int32_t queue_capacity;       /* waiting requests before submit returns RAK_ERR_BUSY [65536] */
+  int32_t reserved;
+  rak_options run;              /* options of every run (layout, mode, slots, tolerance, ...) */
+} rak_server_options;
+
+typedef struct rak_server_stats {
+  uint64_t submitted, completed, rejected, launches, graphs_launched;
+  uint64_t edges_completed;     /* directed edges of completed requests */
+  uint64_t device_bytes_in_use; /* budget currently held by admitted requests */
+  int32_t max_concurrent_launches;
+  int32_t pending;              /* requests waiting for admission */
+} rak_server_stats;
+
+void rak_server_options_default(rak_server_options *o);
+/* Starts the loop on ctx's device. */
+rak_status rak_server_create(rak_ctx *ctx, const rak_server_options *o, rak_server **out);
+/* Queues a host-located graph; its arrays must stay valid and unchanged until the request
+ * completes (page-locked arrays copy fastest). RAK_ERR_BUSY when the queue is full. */
+rak_status rak_server_submit(rak_server *s, const rak_csr *g, uint64_t *ticket);
+/* Waits up to timeout_s for a request (RAK_ERR_TIMEOUT otherwise), then copies its membership
+ * (host, n entries; may be NULL) and result: iterations; time_ms = latency from submit to
+ * completion; plan_ms = time waiting for admission. The ticket is released. A request larger than
+ * the whole budget completes with RAK_ERR_OUT_OF_MEMORY. */
+rak_status rak_server_wait(rak_server *s, uint64_t ticket, double timeout_s, uint32_t *membership,
+                           rak_result *res);
+rak_status rak_server_stats_get(rak_server *s, rak_server_stats *st);
+/* Finishes every queued request, then stops the loop and frees everything. */
+rak_status rak_server_destroy(rak_server *s);
+
 /* ---- a run that allocates no device memory ------------------------------------------------ */
 /* Size of the fixed device array rak_lowmem_cuda_noalloc works in. Every GPU that loads the
  * library holds this many bytes until the process exits. */

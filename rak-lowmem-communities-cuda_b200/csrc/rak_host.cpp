@@ -12,9 +12,16 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <chrono>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
 #include <limits>
+#include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "rak_internal.hpp"
@@ -90,7 +97,11 @@ struct rak_graph {
   rak::Regions rg{};
   uint64_t graph_bytes = 0, plan_bytes = 0;
   float plan_ms = 0, h2d_ms = 0;
+  size_t off_cap = 0, tgt_cap = 0, wt_cap = 0;  // bytes allocated for an owned copy
+  void *wt_alloc = nullptr;                      // owned weight buffer (wt may be null: unit weights)
   rak_host_detail::RunBufs bufs;  // run buffers reused across runs
+  // plan storage (order and split-vertex tables) and its build space, grown only when too small
+  rak_host_detail::DevBuf p_order, p_hub_first, p_chunk_hub, p_keys, p_keys2, p_vids, p_hist, p_temp, p_deg;
 };
 
 struct rak_batch {
@@ -247,61 +258,61 @@ void regions_from(const std::vector<unsigned long long> &hist, const Layout &ly,
 
 rak_status build_plan(rak_ctx *ctx, rak_graph *gr, const Layout &ly, Tracker *tr) {
   cudaStream_t st = ctx->stream;
-  cudaFree(gr->order); gr->order = nullptr;
-  cudaFree(gr->chunk_hub); gr->chunk_hub = nullptr;
-  cudaFree(gr->hub_first); gr->hub_first = nullptr;
-  gr->plan_bytes = 0;
   gr->ly = ly;
   const int64_t n = gr->n;
   const int nk = nkeys_of(ly);
   Events ev;
   cudaEventRecord(ev.e[0], st);
-  DevBuf keys, keys2, vids, hist, temp;
-  RAK_TRY(ctx, keys.alloc(size_t(n) * 4, tr));
-  RAK_TRY(ctx, keys2.alloc(size_t(n) * 4, tr));
-  RAK_TRY(ctx, vids.alloc(size_t(n) * 4, tr));
-  RAK_TRY(ctx, hist.alloc(size_t(nk) * 8, tr));
-  RAK_TRY(ctx, cudaMalloc(&gr->order, size_t(std::max<int64_t>(n, 1)) * 4));
-  gr->plan_bytes += size_t(std::max<int64_t>(n, 1)) * 4;
-  if (tr) tr->add(size_t(std::max<int64_t>(n, 1)) * 4);
-  RAK_TRY(ctx, cudaMemsetAsync(hist.p, 0, size_t(nk) * 8, st));
+  const size_t n4 = size_t(std::max<int64_t>(n, 1)) * 4;
+  RAK_TRY(ctx, ensure(gr->p_order, n4));
+  RAK_TRY(ctx, ensure(gr->p_keys, n4));
+  RAK_TRY(ctx, ensure(gr->p_keys2, n4));
+  RAK_TRY(ctx, ensure(gr->p_vids, n4));
+  RAK_TRY(ctx, ensure(gr->p_hist, size_t(nk) * 8));
+  gr->order = gr->p_order.as<uint32_t>();
+  if (tr) tr->add(n4 * 4 + size_t(nk) * 8);
+  RAK_TRY(ctx, cudaMemsetAsync(gr->p_hist.p, 0, size_t(nk) * 8, st));
   std::vector<unsigned long long> h(size_t(nk), 0);
   if (n > 0) {
-    RAK_TRY(ctx, rak::launch_plan_keys(gr->off, gr->off64, n, ly, keys.as<uint32_t>(), vids.as<uint32_t>(),
-                                       hist.as<unsigned long long>(), nk, st));
+    RAK_TRY(ctx, rak::launch_plan_keys(gr->off, gr->off64, n, ly, gr->p_keys.as<uint32_t>(), gr->p_vids.as<uint32_t>(),
+                                       gr->p_hist.as<unsigned long long>(), nk, st));
     int end_bit = 1;
     while ((1 << end_bit) < nk) ++end_bit;
     size_t tb = 0;
-    RAK_TRY(ctx, rak::plan_sort(keys.as<uint32_t>(), keys2.as<uint32_t>(), vids.as<uint32_t>(), gr->order, n,
-                                end_bit, nullptr, &tb, st));
-    RAK_TRY(ctx, temp.alloc(tb, tr));
-    RAK_TRY(ctx, rak::plan_sort(keys.as<uint32_t>(), keys2.as<uint32_t>(), vids.as<uint32_t>(), gr->order, n,
-                                end_bit, temp.p, &tb, st));
-    RAK_TRY(ctx, cudaMemcpyAsync(h.data(), hist.p, size_t(nk) * 8, cudaMemcpyDeviceToHost, st));
+    RAK_TRY(ctx, rak::plan_sort(gr->p_keys.as<uint32_t>(), gr->p_keys2.as<uint32_t>(), gr->p_vids.as<uint32_t>(),
+                                gr->order, n, end_bit, nullptr, &tb, st));
+    RAK_TRY(ctx, ensure(gr->p_temp, tb));
+    if (tr) tr->add(gr->p_temp.bytes);
+    RAK_TRY(ctx, rak::plan_sort(gr->p_keys.as<uint32_t>(), gr->p_keys2.as<uint32_t>(), gr->p_vids.as<uint32_t>(),
+                                gr->order, n, end_bit, gr->p_temp.p, &tb, st));
+    RAK_TRY(ctx, cudaMemcpyAsync(h.data(), gr->p_hist.p, size_t(nk) * 8, cudaMemcpyDeviceToHost, st));
     RAK_TRY(ctx, cudaStreamSynchronize(st));
   }
   gr->nhub = int64_t(h.empty() ? 0 : h[0]);
   gr->nchunks = 0;
+  gr->hub_first = nullptr;
+  gr->chunk_hub = nullptr;
   std::vector<int64_t> first(size_t(gr->nhub) + 1, 0);
   if (gr->nhub > 0) {
-    DevBuf deg;
-    RAK_TRY(ctx, deg.alloc(size_t(gr->nhub) * 8, tr));
-    RAK_TRY(ctx, rak::launch_hub_degrees(gr->off, gr->off64, gr->order, gr->nhub, deg.as<int64_t>(), st));
+    RAK_TRY(ctx, ensure(gr->p_deg, size_t(gr->nhub) * 8));
+    RAK_TRY(ctx, rak::launch_hub_degrees(gr->off, gr->off64, gr->order, gr->nhub, gr->p_deg.as<int64_t>(), st));
     std::vector<int64_t> hd(size_t(gr->nhub));
-    RAK_TRY(ctx, cudaMemcpyAsync(hd.data(), deg.p, size_t(gr->nhub) * 8, cudaMemcpyDeviceToHost, st));
+    RAK_TRY(ctx, cudaMemcpyAsync(hd.data(), gr->p_deg.p, size_t(gr->nhub) * 8, cudaMemcpyDeviceToHost, st));
     RAK_TRY(ctx, cudaStreamSynchronize(st));
     for (int64_t i = 0; i < gr->nhub; ++i) first[i + 1] = first[i] + (hd[i] + ly.hub_chunk - 1) / ly.hub_chunk;
     gr->nchunks = first[gr->nhub];
     std::vector<uint32_t> ch(size_t(gr->nchunks));
     for (int64_t i = 0; i < gr->nhub; ++i)
       for (int64_t c = first[i]; c < first[i + 1]; ++c) ch[c] = uint32_t(i);
-    RAK_TRY(ctx, cudaMalloc(&gr->hub_first, first.size() * 8));
-    RAK_TRY(ctx, cudaMalloc(&gr->chunk_hub, ch.size() * 4));
-    gr->plan_bytes += first.size() * 8 + ch.size() * 4;
+    RAK_TRY(ctx, ensure(gr->p_hub_first, first.size() * 8));
+    RAK_TRY(ctx, ensure(gr->p_chunk_hub, ch.size() * 4));
+    gr->hub_first = gr->p_hub_first.as<int64_t>();
+    gr->chunk_hub = gr->p_chunk_hub.as<uint32_t>();
     if (tr) tr->add(first.size() * 8 + ch.size() * 4);
     RAK_TRY(ctx, cudaMemcpyAsync(gr->hub_first, first.data(), first.size() * 8, cudaMemcpyHostToDevice, st));
     RAK_TRY(ctx, cudaMemcpyAsync(gr->chunk_hub, ch.data(), ch.size() * 4, cudaMemcpyHostToDevice, st));
   }
+  gr->plan_bytes = gr->p_order.bytes + gr->p_hub_first.bytes + gr->p_chunk_hub.bytes;
   regions_from(h, ly, gr->nchunks, &gr->rg);
   cudaEventRecord(ev.e[1], st);
   RAK_TRY(ctx, cudaStreamSynchronize(st));
@@ -341,6 +352,10 @@ rak_status graph_create(rak_ctx *ctx, const rak_csr *g, const Resolved &r, Track
     if (e == cudaSuccess) e = cudaMalloc(&pt, size_t(std::max<int64_t>(g->m, 1)) * 4);
     if (e == cudaSuccess && g->weights) e = cudaMalloc(&pw, size_t(std::max<int64_t>(g->m, 1)) * 4);
     gr->off = po; gr->tgt = static_cast<uint32_t *>(pt); gr->wt = static_cast<float *>(pw);
+    gr->off_cap = ob;
+    gr->tgt_cap = size_t(std::max<int64_t>(g->m, 1)) * 4;
+    gr->wt_cap = g->weights ? gr->tgt_cap : 0;
+    gr->wt_alloc = pw;
     if (e != cudaSuccess) return fail(from_cuda(ctx, e, "cudaMalloc(graph)"));
     gr->graph_bytes = ob + size_t(std::max<int64_t>(g->m, 1)) * 4 * (g->weights ? 2 : 1);
     if (tr) tr->add(gr->graph_bytes);
@@ -564,11 +579,8 @@ rak_status rak_graph_destroy(rak_graph *gr) {
   if (gr->owns) {
     cudaFree(const_cast<void *>(gr->off));
     cudaFree(const_cast<uint32_t *>(gr->tgt));
-    cudaFree(const_cast<float *>(gr->wt));
+    cudaFree(gr->wt_alloc);
   }
-  cudaFree(gr->order);
-  cudaFree(gr->chunk_hub);
-  cudaFree(gr->hub_first);
   delete gr;
   return RAK_OK;
 }
@@ -799,7 +811,8 @@ rak_status batch_prepare(rak_ctx *ctx, rak_batch *b, const Resolved &r) {
 
 // Enqueues the whole run; buffers must already be prepared (no allocation here, so the sequence
 // is capturable).
-rak_status batch_enqueue(rak_ctx *ctx, rak_batch *b, const uint32_t *q, const Resolved &r, uint32_t *membership) {
+rak_status batch_enqueue(rak_ctx *ctx, rak_batch *b, const uint32_t *q, const Resolved &r, uint32_t *membership,
+                         int grid_cap = 0) {
   rak_graph *gr = b->g;
   RunBufs &rb = gr->bufs;
   cudaStream_t st = ctx->stream;
@@ -829,7 +842,7 @@ rak_status batch_enqueue(rak_ctx *ctx, rak_batch *b, const uint32_t *q, const Re
     a.stats = rb.stats.as<unsigned long long>(); a.rs = rb.rs.p;
     a.gid = b->gid.as<uint32_t>(); a.vbase = b->vbase.as<int64_t>(); a.gdone = b->gdone.as<uint8_t>();
     a.giters = b->giters.as<int32_t>(); a.gchanged = b->gchanged.as<unsigned long long>();
-    a.running = b->running.as<unsigned int>(); a.ngraphs = G;
+    a.running = b->running.as<unsigned int>(); a.ngraphs = G; a.grid_cap = grid_cap;
     a.iters = r.iters; a.start_iter = r.start; a.tolerance = r.tol; a.pickless_step = r.pickless;
     a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.timeout_ns = 20LL * 1000 * 1000 * 1000;
     int grid = 0;
@@ -1010,6 +1023,406 @@ rak_status rak_batch_modularity_f64(rak_ctx *ctx, rak_batch *b, const uint32_t *
     const double in = h[size_t(gi)], tot = h[size_t(G + gi)], sq = h[size_t(2 * G + gi)];
     q[gi] = tot > 0 ? in / tot - sq / (tot * tot) : 0.0;
   }
+  return RAK_OK;
+}
+
+}  // extern "C"
+
+// ---- serving: continuous batching -----------------------------------------------------------
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct ServerRequest {
+  uint64_t ticket = 0;
+  rak_csr g{};        // the caller's host arrays (valid until completion)
+  uint64_t bytes = 0; // budget held while admitted
+  Clock::time_point t_submit, t_launch, t_done;
+  std::vector<uint32_t> membership;
+  int32_t iterations = 0;
+  rak_status status = RAK_OK;
+  bool done = false;
+};
+using ReqPtr = std::shared_ptr<ServerRequest>;
+
+// Page-locked host buffer, grown only when too small.
+struct Pinned {
+  void *p = nullptr;
+  size_t bytes = 0;
+  Pinned() = default;
+  Pinned(const Pinned &) = delete;
+  Pinned &operator=(const Pinned &) = delete;
+  ~Pinned() { if (p) cudaFreeHost(p); }
+  cudaError_t ensure(size_t b) {
+    if (p && bytes >= b) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    const size_t want = b + b / 2 + 4096;
+    cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+    if (e == cudaSuccess) bytes = want;
+    else p = nullptr;
+    return e;
+  }
+  template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+// One launch slot: its own context (stream), a reusable batch and staging buffers.
+struct ServerSlot {
+  rak_ctx *ctx = nullptr;
+  rak_batch *b = nullptr;
+  Pinned h_go, h_off, h_mem, h_it;
+  DevBuf d_mem;
+  cudaEvent_t ev = nullptr;
+  std::vector<ReqPtr> reqs;
+  std::vector<int64_t> vo;
+  bool busy = false;       // holds requests
+  bool launching = false;  // requests taken, event not recorded yet
+};
+
+// Budget charged for a request: its graph plus per-vertex labels, flags and plan.
+uint64_t request_bytes(const rak_csr &g) {
+  const uint64_t n = uint64_t(g.n), m = uint64_t(g.m);
+  return 8 * (n + 1) + 4 * m + (g.weights ? 4 * m : 0) + 32 * n + 256;
+}
+
+// Grows an owned device array of a graph (contents are not kept).
+cudaError_t grow(const void *&p, size_t &cap, size_t need) {
+  if (p && cap >= need) return cudaSuccess;
+  cudaFree(const_cast<void *>(p));
+  p = nullptr;
+  cap = 0;
+  void *q = nullptr;
+  const size_t want = need + need / 2 + 256;
+  cudaError_t e = cudaMalloc(&q, want);
+  if (e != cudaSuccess) return e;
+  p = q;
+  cap = want;
+  return cudaSuccess;
+}
+
+}  // namespace
+
+struct rak_server {
+  rak_ctx *ctx = nullptr;
+  int device = 0;
+  rak_server_options opt{};
+  Resolved run{};
+  int grid_cap = 0;
+  std::thread worker;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<ReqPtr> pending;
+  std::unordered_map<uint64_t, ReqPtr> tickets;
+  std::vector<std::unique_ptr<ServerSlot>> slots;
+  uint64_t used = 0, next_ticket = 1;
+  bool stop = false;
+  rak_server_stats st{};
+};
+
+namespace {
+
+// Packs the slot's requests into its batch on the device: offsets rebased on the host into
+// page-locked staging, targets and weights copied straight from the callers' arrays.
+rak_status server_load(rak_server *s, ServerSlot &sl) {
+  rak_ctx *ctx = sl.ctx;
+  cudaStream_t st = ctx->stream;
+  const size_t G = sl.reqs.size();
+  sl.vo.assign(G + 1, 0);
+  int64_t m_tot = 0;
+  bool weighted = false;
+  for (size_t i = 0; i < G; ++i) {
+    sl.vo[i + 1] = sl.vo[i] + sl.reqs[i]->g.n;
+    m_tot += sl.reqs[i]->g.m;
+    weighted |= sl.reqs[i]->g.weights != nullptr;
+  }
+  const int64_t n_tot = sl.vo[G];
+  RAK_TRY(ctx, sl.h_go.ensure((G + 1) * 8));
+  RAK_TRY(ctx, sl.h_off.ensure(size_t(n_tot + 1) * 8));
+  int64_t *go = sl.h_go.as<int64_t>(), *off = sl.h_off.as<int64_t>();
+  int64_t e_base = 0;
+  for (size_t i = 0; i < G; ++i) {
+    go[i] = sl.vo[i];
+    const rak_csr &g = sl.reqs[i]->g;
+    int64_t *o = off + sl.vo[i];
+    if (g.offset_bits == 64) {
+      const int64_t *src = static_cast<const int64_t *>(g.offsets);
+      for (int64_t u = 0; u < g.n; ++u) o[u] = src[u] + e_base;
+    } else {
+      const int32_t *src = static_cast<const int32_t *>(g.offsets);
+      for (int64_t u = 0; u < g.n; ++u) o[u] = int64_t(src[u]) + e_base;
+    }
+    e_base += g.m;
+  }
+  go[G] = n_tot;
+  off[n_tot] = m_tot;
+  if (!sl.b) {
+    auto *b = new (std::nothrow) rak_batch();
+    auto *gr = new (std::nothrow) rak_graph();
+    if (!b || !gr) { delete b; delete gr; return RAK_ERR_OUT_OF_MEMORY; }
+    gr->ctx = ctx;
+    gr->device = ctx->device;
+    gr->owns = true;
+    gr->off64 = true;
+    b->ctx = ctx;
+    b->device = ctx->device;
+    b->g = gr;
+    sl.b = b;
+  }
+  rak_batch *b = sl.b;
+  rak_graph *gr = b->g;
+  RAK_TRY(ctx, grow(gr->off, gr->off_cap, size_t(n_tot + 1) * 8));
+  const void *tp = gr->tgt;
+  RAK_TRY(ctx, grow(tp, gr->tgt_cap, size_t(std::max<int64_t>(m_tot, 1)) * 4));
+  gr->tgt = static_cast<const uint32_t *>(tp);
+  if (weighted) {
+    const void *wp = gr->wt_alloc;
+    RAK_TRY(ctx, grow(wp, gr->wt_cap, size_t(std::max<int64_t>(m_tot, 1)) * 4));
+    gr->wt_alloc = const_cast<void *>(wp);
+  }
+  gr->n = n_tot;
+  gr->m = m_tot;
+  gr->wt = weighted ? static_cast<const float *>(gr->wt_alloc) : nullptr;
+  gr->graph_bytes = gr->off_cap + gr->tgt_cap + gr->wt_cap;
+  RAK_TRY(ctx, cudaMemcpyAsync(const_cast<void *>(gr->off), off, size_t(n_tot + 1) * 8, cudaMemcpyHostToDevice, st));
+  e_base = 0;
+  for (size_t i = 0; i < G; ++i) {
+    const rak_csr &g = sl.reqs[i]->g;
+    if (g.m > 0) {
+      RAK_TRY(ctx, cudaMemcpyAsync(const_cast<uint32_t *>(gr->tgt) + e_base, g.targets, size_t(g.m) * 4,
+                                   cudaMemcpyHostToDevice, st));
+      float *w = static_cast<float *>(gr->wt_alloc) + e_base;
+      if (weighted && g.weights) RAK_TRY(ctx, cudaMemcpyAsync(w, g.weights, size_t(g.m) * 4, cudaMemcpyHostToDevice, st));
+      else if (weighted) RAK_TRY(ctx, rak::launch_fill_f32(w, g.m, 1.0f, st));
+    }
+    e_base += g.m;
+  }
+  b->ngraphs = int64_t(G);
+  RAK_TRY(ctx, ensure(b->vbase, (G + 1) * 8));
+  RAK_TRY(ctx, cudaMemcpyAsync(b->vbase.p, go, (G + 1) * 8, cudaMemcpyHostToDevice, st));
+  RAK_TRY(ctx, ensure(b->gid, size_t(std::max<int64_t>(n_tot, 1)) * 4));
+  RAK_TRY(ctx, rak::launch_batch_gid(b->vbase.as<int64_t>(), int64_t(G), b->gid.as<uint32_t>(), st));
+  return build_plan(ctx, gr, s->run.ly, nullptr);
+}
+
+rak_status server_launch(rak_server *s, ServerSlot &sl) {
+  RAK_CHECK(server_load(s, sl));
+  rak_ctx *ctx = sl.ctx;
+  rak_batch *b = sl.b;
+  const int64_t n = b->g->n, G = b->ngraphs;
+  RAK_CHECK(batch_prepare(ctx, b, s->run));
+  RAK_TRY(ctx, ensure(sl.d_mem, size_t(std::max<int64_t>(n, 1)) * 4));
+  RAK_TRY(ctx, sl.h_mem.ensure(size_t(std::max<int64_t>(n, 1)) * 4));
+  RAK_TRY(ctx, sl.h_it.ensure(size_t(std::max<int64_t>(G, 1)) * 4));
+  RAK_CHECK(batch_enqueue(ctx, b, nullptr, s->run, sl.d_mem.as<uint32_t>(), s->grid_cap));
+  RAK_TRY(ctx, cudaMemcpyAsync(sl.h_mem.p, sl.d_mem.p, size_t(n) * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  RAK_TRY(ctx, cudaMemcpyAsync(sl.h_it.p, b->giters.p, size_t(G) * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  RAK_TRY(ctx, cudaEventRecord(sl.ev, ctx->stream));
+  return RAK_OK;
+}
+
+void server_loop(rak_server *s) {
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  for (;;) {
+    int inflight = 0;
+    for (auto &slp : s->slots) {
+      ServerSlot &sl = *slp;
+      if (!sl.busy || sl.launching) { inflight += sl.busy; continue; }
+      if (cudaEventQuery(sl.ev) != cudaSuccess) { ++inflight; continue; }
+      const auto now = Clock::now();
+      const uint32_t *mem = sl.h_mem.as<uint32_t>();
+      const int32_t *its = sl.h_it.as<int32_t>();
+      for (size_t i = 0; i < sl.reqs.size(); ++i) {
+        ServerRequest &r = *sl.reqs[i];
+        r.membership.assign(mem + sl.vo[i], mem + sl.vo[i + 1]);
+        r.iterations = its[i];
+        r.t_done = now;
+        r.done = true;
+        s->used -= r.bytes;
+        s->st.completed++;
+        s->st.edges_completed += uint64_t(r.g.m);
+      }
+      sl.reqs.clear();
+      sl.busy = false;
+      s->cv_done.notify_all();
+    }
+    ServerSlot *free_slot = nullptr;
+    for (auto &slp : s->slots)
+      if (!slp->busy) { free_slot = slp.get(); break; }
+    if (free_slot && !s->pending.empty()) {
+      std::vector<ReqPtr> sel;
+      uint64_t bytes = 0;
+      while (!s->pending.empty() && int(sel.size()) < s->opt.max_graphs_per_launch) {
+        ReqPtr r = s->pending.front();
+        if (r->bytes > s->opt.budget_bytes) {  // can never fit
+          s->pending.pop_front();
+          r->status = RAK_ERR_OUT_OF_MEMORY;
+          r->done = true;
+          r->t_done = Clock::now();
+          s->st.rejected++;
+          s->cv_done.notify_all();
+          continue;
+        }
+        if (s->used + bytes + r->bytes > s->opt.budget_bytes) break;
+        sel.push_back(r);
+        bytes += r->bytes;
+        s->pending.pop_front();
+      }
+      if (!sel.empty()) {
+        s->used += bytes;
+        const auto now = Clock::now();
+        for (auto &r : sel) r->t_launch = now;
+        free_slot->reqs = std::move(sel);
+        free_slot->busy = true;
+        free_slot->launching = true;
+        s->st.launches++;
+        s->st.graphs_launched += free_slot->reqs.size();
+        s->st.max_concurrent_launches = std::max(s->st.max_concurrent_launches, inflight + 1);
+        lk.unlock();
+        const rak_status rs = server_launch(s, *free_slot);
+        lk.lock();
+        free_slot->launching = false;
+        if (rs != RAK_OK) {
+          for (auto &r : free_slot->reqs) {
+            r->status = rs;
+            r->done = true;
+            r->t_done = Clock::now();
+            s->used -= r->bytes;
+          }
+          free_slot->reqs.clear();
+          free_slot->busy = false;
+          s->cv_done.notify_all();
+        }
+        continue;
+      }
+    }
+    if (s->stop && s->pending.empty() && inflight == 0) break;
+    s->cv_work.wait_for(lk, std::chrono::microseconds(inflight > 0 ? 50 : 1000));
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void rak_server_options_default(rak_server_options *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->budget_bytes = uint64_t(16) << 30;
+  o->max_graphs_per_launch = 256;
+  o->slots = 2;
+  o->queue_capacity = 65536;
+  rak_options_default(&o->run);
+}
+
+rak_status rak_server_create(rak_ctx *ctx, const rak_server_options *o, rak_server **out) {
+  if (!ctx || !out) return RAK_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  rak_server_options d;
+  rak_server_options_default(&d);
+  if (!o) o = &d;
+  if (o->slots < 1 || o->slots > 16 || o->max_graphs_per_launch < 1 || o->queue_capacity < 1) {
+    set_err(ctx, "server options out of range");
+    return RAK_ERR_INVALID_ARGUMENT;
+  }
+  auto *s = new (std::nothrow) rak_server();
+  if (!s) return RAK_ERR_OUT_OF_MEMORY;
+  s->ctx = ctx;
+  s->device = ctx->device;
+  s->opt = *o;
+  rak_status st = resolve(ctx, &o->run, &s->run);
+  if (st != RAK_OK) { delete s; return st; }
+  s->grid_cap = std::max(1, ctx->sms * 3 / o->slots);
+  for (int i = 0; i < o->slots; ++i) {
+    s->slots.push_back(std::make_unique<ServerSlot>());
+    ServerSlot &sl = *s->slots.back();
+    st = rak_ctx_create(ctx->device, &sl.ctx);
+    if (st == RAK_OK && cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) != cudaSuccess) st = RAK_ERR_CUDA;
+    if (st != RAK_OK) {
+      for (auto &x : s->slots) { if (x->ev) cudaEventDestroy(x->ev); if (x->ctx) rak_ctx_destroy(x->ctx); }
+      delete s;
+      return st;
+    }
+  }
+  s->worker = std::thread(server_loop, s);
+  *out = s;
+  return RAK_OK;
+}
+
+rak_status rak_server_submit(rak_server *s, const rak_csr *g, uint64_t *ticket) {
+  if (!s || !g || !ticket) return RAK_ERR_INVALID_ARGUMENT;
+  if (check_csr_shape(nullptr, g) != RAK_OK || g->location != RAK_HOST) return RAK_ERR_INVALID_ARGUMENT;
+  if (s->run.validate && rak_csr_validate_host(g) != RAK_OK) return RAK_ERR_INVALID_CSR;
+  auto r = std::make_shared<ServerRequest>();
+  r->g = *g;
+  r->bytes = request_bytes(*g);
+  r->t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) return RAK_ERR_INVALID_ARGUMENT;
+    if (int64_t(s->pending.size()) >= s->opt.queue_capacity) return RAK_ERR_BUSY;
+    r->ticket = s->next_ticket++;
+    s->tickets[r->ticket] = r;
+    s->pending.push_back(r);
+    s->st.submitted++;
+  }
+  s->cv_work.notify_one();
+  *ticket = r->ticket;
+  return RAK_OK;
+}
+
+rak_status rak_server_wait(rak_server *s, uint64_t ticket, double timeout_s, uint32_t *membership, rak_result *res) {
+  if (!s) return RAK_ERR_INVALID_ARGUMENT;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->tickets.find(ticket);
+  if (it == s->tickets.end()) return RAK_ERR_INVALID_ARGUMENT;
+  ReqPtr r = it->second;
+  const auto limit = std::chrono::duration<double>(timeout_s < 0 ? 0.0 : timeout_s);
+  if (!s->cv_done.wait_for(lk, limit, [&] { return r->done; })) return RAK_ERR_TIMEOUT;
+  s->tickets.erase(it);
+  lk.unlock();
+  if (res) {
+    std::memset(res, 0, sizeof(*res));
+    res->modularity = std::numeric_limits<double>::quiet_NaN();
+    res->iterations = r->iterations;
+    res->time_ms = float(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
+    const auto started = r->status == RAK_OK ? r->t_launch : r->t_done;
+    res->plan_ms = float(std::chrono::duration<double, std::milli>(started - r->t_submit).count());
+  }
+  if (r->status != RAK_OK) return r->status;
+  if (membership && !r->membership.empty()) std::memcpy(membership, r->membership.data(), r->membership.size() * 4);
+  return RAK_OK;
+}
+
+rak_status rak_server_stats_get(rak_server *s, rak_server_stats *out) {
+  if (!s || !out) return RAK_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(s->mu);
+  *out = s->st;
+  out->device_bytes_in_use = s->used;
+  out->pending = int32_t(s->pending.size());
+  return RAK_OK;
+}
+
+rak_status rak_server_destroy(rak_server *s) {
+  if (!s) return RAK_ERR_INVALID_ARGUMENT;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  cudaSetDevice(s->device);
+  for (auto &slp : s->slots) {
+    ServerSlot &sl = *slp;
+    if (sl.ctx) cudaStreamSynchronize(sl.ctx->stream);
+    if (sl.b) rak_batch_destroy(sl.b);
+    sl.d_mem.release();
+    if (sl.ev) cudaEventDestroy(sl.ev);
+    if (sl.ctx) rak_ctx_destroy(sl.ctx);
+  }
+  delete s;
   return RAK_OK;
 }
 

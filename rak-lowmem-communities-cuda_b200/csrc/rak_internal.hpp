@@ -84,6 +84,7 @@ struct LpaArgs {
   unsigned long long *gchanged; // 2*ngraphs: vertices changed per graph, this and next iteration
   unsigned int *running;        // per iteration: graphs still running after it
   int64_t ngraphs;
+  int grid_cap;                 // at most this many blocks (0: as many as fit), to share the GPU
   int iters;
   int start_iter;
   double tolerance;
@@ -123,6 +124,7 @@ cudaError_t launch_modularity(const void *off, bool off64, const uint32_t *tgt, 
                               cudaStream_t st);
 
 // Batches of graphs (rak_kernels.cu).
+cudaError_t launch_fill_f32(float *p, int64_t count, float v, cudaStream_t st);
 cudaError_t launch_batch_gid(const int64_t *vbase, int64_t ngraphs, uint32_t *gid, cudaStream_t st);
 cudaError_t launch_batch_validate(const int64_t *vbase, int64_t ngraphs, int64_t n, const int64_t *off,
                                   const uint32_t *tgt, const uint32_t *gid, unsigned int *bad, cudaStream_t st);

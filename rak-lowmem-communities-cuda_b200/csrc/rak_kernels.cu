@@ -211,7 +211,17 @@ __global__ void k_batch_mod_square(const double *ctot, const uint32_t *gid, int6
     if (ctot[c] != 0.0) atomicAdd(gsq + gid[c], ctot[c] * ctot[c]);
 }
 
+__global__ void k_fill_f32(float *p, int64_t count, float v) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = tid; i < count; i += nt) p[i] = v;
+}
+
 }  // namespace
+
+cudaError_t launch_fill_f32(float *p, int64_t count, float v, cudaStream_t st) {
+  k_fill_f32<<<grid_for(count, 4), TPB, 0, st>>>(p, count, v);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_batch_gid(const int64_t *vbase, int64_t ngraphs, uint32_t *gid, cudaStream_t st) {
   k_batch_gid<<<grid_for(ngraphs), TPB, 0, st>>>(vbase, ngraphs, gid);

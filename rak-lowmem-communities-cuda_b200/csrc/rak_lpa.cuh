@@ -569,6 +569,7 @@ cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, bool batch,
   int64_t grid = int64_t(per_sm) * sms;
   const int64_t want = (warps_needed + 7) / 8;
   if (want < grid) grid = want;
+  if (a.grid_cap > 0 && grid > a.grid_cap) grid = a.grid_cap;
   if (grid < 1) grid = 1;
   if (grid_out) *grid_out = int(grid);
   // Cooperative attribute through cudaLaunchKernelEx: co-residency is guaranteed (the grid

@@ -61,6 +61,18 @@ class rak_batch_csr(C.Structure):
                 ("targets", C.c_void_p), ("weights", C.c_void_p)]
 
 
+class rak_server_options(C.Structure):
+    _fields_ = [("budget_bytes", C.c_uint64), ("max_graphs_per_launch", C.c_int32), ("slots", C.c_int32),
+                ("queue_capacity", C.c_int32), ("reserved", C.c_int32), ("run", rak_options)]
+
+
+class rak_server_stats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("rejected", C.c_uint64),
+                ("launches", C.c_uint64), ("graphs_launched", C.c_uint64), ("edges_completed", C.c_uint64),
+                ("device_bytes_in_use", C.c_uint64), ("max_concurrent_launches", C.c_int32),
+                ("pending", C.c_int32)]
+
+
 class rak_host_csr(C.Structure):
     _fields_ = [("n", C.c_int64), ("m", C.c_int64), ("offsets", C.c_void_p), ("targets", C.c_void_p),
                 ("weights", C.c_void_p), ("truth", C.c_void_p)]
@@ -95,6 +107,12 @@ _sig("rak_batch_results", C.c_int, P, P, P, C.POINTER(rak_result))
 _sig("rak_batch_capture", C.c_int, P, P, P, C.POINTER(rak_options), P)
 _sig("rak_batch_replay", C.c_int, P, P)
 _sig("rak_batch_modularity_f64", C.c_int, P, P, P, P)
+_sig("rak_server_options_default", None, C.POINTER(rak_server_options))
+_sig("rak_server_create", C.c_int, P, C.POINTER(rak_server_options), C.POINTER(P))
+_sig("rak_server_submit", C.c_int, P, C.POINTER(rak_csr), C.POINTER(C.c_uint64))
+_sig("rak_server_wait", C.c_int, P, C.c_uint64, C.c_double, P, C.POINTER(rak_result))
+_sig("rak_server_stats_get", C.c_int, P, C.POINTER(rak_server_stats))
+_sig("rak_server_destroy", C.c_int, P)
 _sig("rak_lowmem_cuda_noalloc", C.c_int, C.c_int, P, C.POINTER(rak_csr), P, C.POINTER(rak_options), P,
      C.POINTER(rak_result))
 NOALLOC_SCRATCH_BYTES = 64 << 20
@@ -476,6 +494,55 @@ class Batch:
         _check(_lib.rak_batch_modularity_f64(self.ctx.handle, self._b, membership.data_ptr(), q.ctypes.data),
                self.ctx.handle)
         return q[:self.graphs]
+
+
+class Server:
+    """Continuous-batching request loop (rak_server_*). submit() takes host graphs, which must stay
+    alive and unchanged until wait() returns for them (the object keeps a reference)."""
+
+    def __init__(self, ctx: Context, budget_bytes=16 << 30, max_graphs_per_launch=256, slots=2,
+                 queue_capacity=65536, **run_opts):
+        o = rak_server_options()
+        _lib.rak_server_options_default(C.byref(o))
+        o.budget_bytes, o.max_graphs_per_launch, o.slots, o.queue_capacity = \
+            budget_bytes, max_graphs_per_launch, slots, queue_capacity
+        o.run = options(**run_opts)
+        self.ctx = ctx
+        self._s = P()
+        self._keep = {}
+        _check(_lib.rak_server_create(ctx.handle, C.byref(o), C.byref(self._s)), ctx.handle)
+
+    def submit(self, g: HostGraph) -> int:
+        c = g.csr()
+        t = C.c_uint64(0)
+        _check(_lib.rak_server_submit(self._s, C.byref(c), C.byref(t)))
+        self._keep[t.value] = g
+        return t.value
+
+    def wait(self, ticket: int, timeout=120.0):
+        g = self._keep.get(ticket)
+        out = np.empty(g.n if g is not None else 0, dtype=np.uint32)
+        r = rak_result()
+        st = _lib.rak_server_wait(self._s, ticket, timeout, out.ctypes.data if len(out) else None, C.byref(r))
+        if st != 5:                      # not a timeout: the ticket is released
+            self._keep.pop(ticket, None)
+        if st != 0:
+            raise RakError(st)
+        return out, Result.of(r)
+
+    def stats(self) -> dict:
+        st = rak_server_stats()
+        _check(_lib.rak_server_stats_get(self._s, C.byref(st)))
+        return {f[0]: getattr(st, f[0]) for f in rak_server_stats._fields_}
+
+    def close(self):
+        if self._s and _lib is not None:
+            _lib.rak_server_destroy(self._s)
+            self._s = P()
+        self._keep = {}
+
+    def __del__(self):
+        self.close()
 
 
 def write_rakcsr(path: str, g: HostGraph):

@@ -1,0 +1,109 @@
+"""Serving loop (rak_server_*): continuous batching with admission by a device-memory budget and
+overlapping launches. Each request's result must be the same in the mix as alone (synchronous
+mode: identical labels and iterations; asynchronous mode: the planted partitions recovered to
+the same quality), oversized requests are refused, and a full queue answers busy."""
+import threading
+
+import numpy as np
+import pytest
+
+import rak_lowmem as rl
+
+pytestmark = pytest.mark.gpu
+
+LAYOUT = dict(lane_max=8, hub_min=64, hub_chunk=32)
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = rl.Context(0)
+    yield c
+    c.close()
+
+
+def request_graphs():
+    gs = [rl.gen_rmat(s, 6, seed=200 + s) for s in (8, 11, 9, 12, 10)]
+    gs += [rl.gen_rmat(10, 8, seed=7, w_lo=1.0, w_hi=5.0), rl.gen_sbm(3000, 20, 12.0, 20.0, seed=3),
+           rl.gen_lattice(30, 20, 0.05, 0.02, seed=4), rl.HostGraph(np.zeros(3, np.int64), np.zeros(0, np.uint32))]
+    return gs * 3
+
+
+def test_results_same_alone_and_in_the_mix(ctx):
+    gs = request_graphs()
+    alone = [ctx.lowmem(g, mode=rl.MODE_SYNC, **LAYOUT) for g in gs]
+    srv = rl.Server(ctx, budget_bytes=64 << 20, max_graphs_per_launch=5, slots=2, mode=rl.MODE_SYNC, **LAYOUT)
+    tickets = [None] * len(gs)
+
+    def client(idx):
+        for i in idx:
+            tickets[i] = srv.submit(gs[i])
+
+    th = [threading.Thread(target=client, args=(range(k, len(gs), 2),)) for k in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for i, g in enumerate(gs):
+        lab, res = srv.wait(tickets[i])
+        np.testing.assert_array_equal(lab, alone[i][0], err_msg=f"request {i}")
+        assert res.iterations == alone[i][1].iterations
+        assert res.time_ms >= res.plan_ms >= 0
+    st = srv.stats()
+    assert st["completed"] == st["submitted"] == len(gs) and st["rejected"] == 0
+    assert st["launches"] >= len(gs) // 5 and st["device_bytes_in_use"] == 0
+    srv.close()
+
+
+def test_async_quality_in_the_mix(ctx):
+    gs = [rl.gen_sbm(4000 + 1000 * k, 20, 16.0, 1000.0, seed=k) for k in range(8)]
+    srv = rl.Server(ctx, max_graphs_per_launch=3, slots=2)
+    ts = [srv.submit(g) for g in gs]
+    import oracle as orc
+    for t, g in zip(ts, gs):
+        lab, res = srv.wait(t)
+        assert lab.max() < g.n and res.iterations >= 1
+        planted = orc.modularity(orc.Graph.of(g), g.truth)
+        assert orc.modularity(orc.Graph.of(g), lab) >= 0.9 * planted
+    srv.close()
+
+
+def test_launches_overlap_under_load(ctx):
+    gs = [rl.gen_rmat(14, 16, seed=300 + i) for i in range(6)]
+    srv = rl.Server(ctx, max_graphs_per_launch=1, slots=2)
+    ts = [srv.submit(g) for g in gs * 4]
+    for t in ts:
+        srv.wait(t)
+    st = srv.stats()
+    assert st["launches"] == len(ts) and st["max_concurrent_launches"] == 2
+    srv.close()
+
+
+def test_oversized_request_refused_others_served(ctx):
+    big = rl.gen_rmat(14, 16, seed=1)
+    small = rl.gen_rmat(7, 4, seed=2)
+    srv = rl.Server(ctx, budget_bytes=1 << 20, slots=1)
+    tb, ts = srv.submit(big), srv.submit(small)
+    with pytest.raises(rl.RakError) as e:
+        srv.wait(tb)
+    assert e.value.status == 3
+    lab, _ = srv.wait(ts)
+    assert len(lab) == small.n
+    assert srv.stats()["rejected"] == 1
+    srv.close()
+
+
+def test_full_queue_is_busy(ctx):
+    first = rl.gen_rmat(16, 16, seed=5)
+    small = rl.gen_rmat(6, 4, seed=6)
+    srv = rl.Server(ctx, max_graphs_per_launch=1, slots=1, queue_capacity=2)
+    tickets, busy = [srv.submit(first)], 0
+    for _ in range(20):
+        try:
+            tickets.append(srv.submit(small))
+        except rl.RakError as e:
+            assert e.status == 8
+            busy += 1
+    assert busy > 0
+    for t in tickets:
+        srv.wait(t)
+    srv.close()
