@@ -321,6 +321,116 @@ def batched_leg(ctx, count, steps, threads, stream):
             "loop_nmi_sbm_mean": float(np.mean(nmis_loop)) if nmis_loop else None}
 
 
+def serving_leg(ctx, rates, seconds, threads, seed=11):
+    """Serving loop (rak_server_*) under Poisson arrivals: 98% of requests draw a graph from a pool
+    of 64 graphs of the batched-launch mix, 2% are a symmetric R-MAT scale 22 / edge factor 16.
+    Two arms per rate: "arena" -- every graph kept in device memory and submitted as a device CSR
+    (packed by a device-to-device gather) -- and "host" -- page-locked host graphs uploaded per
+    request. Latency is submit-to-result per request (measured by the server); graphs/s and edges/s
+    over the span from the first submission to the last result. Quality: the modularity of each
+    served result against the same graph run alone through rak_lowmem_cuda."""
+    import threading
+    import torch
+    import rak_lowmem as rl
+    t0 = time.time()
+    pool = batch_mix(64, seed, threads)
+    big = rl.gen_rmat(22, 16, seed=seed * 7919, threads=threads)
+    graphs = pool + [big]
+    log(f"[serving] pool of {len(pool)} + scale-22 R-MAT ({big.m} edges) generated in {time.time() - t0:.1f}s")
+    assert all(rl.validate_host(g) == 0 for g in graphs)
+    q_alone = [ctx.modularity(g, ctx.lowmem(g)[0]) for g in graphs]
+    q_again = [ctx.modularity(g, ctx.lowmem(g)[0]) for g in graphs]   # control: alone, run again
+
+    def quality(q_of):
+        """Served (or repeated) modularity against the first run alone: the edge-weighted ratio,
+        and how many graphs with Q >= 0.05 land within 0.5% (relative); |dQ| for the others."""
+        ks = sorted(q_of)
+        big = [k for k in ks if q_alone[k] >= 0.05]
+        rel = [abs(q_of[k] - q_alone[k]) / q_alone[k] for k in big]
+        return {"q_ratio_edge_weighted": sum(graphs[k].m * q_of[k] for k in ks) /
+                                         sum(graphs[k].m * q_alone[k] for k in ks),
+                "within_0.5pct": int(sum(r <= 0.005 for r in rel)), "graphs_q_ge_0.05": len(big),
+                "rel_diff_max": float(max(rel)) if rel else None,
+                "abs_diff_max_q_lt_0.05": float(max([abs(q_of[k] - q_alone[k]) for k in ks if k not in big],
+                                                    default=0.0))}
+
+    control = quality({k: q_again[k] for k in range(len(graphs))})
+    arena = []
+    for g in graphs:
+        off = torch.from_numpy(np.ascontiguousarray(g.offsets)).cuda()
+        tgt = torch.from_numpy(g.targets.view(np.int32)).cuda()
+        arena.append(((off, tgt), rl.device_csr(off, tgt, None)))
+    cudart = torch.cuda.cudart()
+    registered = []
+    for g in graphs:
+        for a in (g.offsets, g.targets):
+            if a.nbytes:
+                assert int(cudart.cudaHostRegister(a.ctypes.data, a.nbytes, 0)) == 0, "cudaHostRegister failed"
+                registered.append(a)
+    arms = {}
+    try:
+        for arm in ("arena", "host"):
+            for rate in rates:
+                rng = np.random.default_rng(seed * 1000 + rate)
+                count = max(1, int(round(rate * seconds)))
+                arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
+                picks = np.where(rng.random(count) < 0.02, len(pool), rng.integers(0, len(pool), count))
+                srv = rl.Server(ctx, slots=2, validate=0)
+                tickets = [None] * count
+                lat, queued, done_at, labels = [], [], [0.0] * count, {}
+                ready = threading.Semaphore(0)
+
+                def waiter():
+                    for i in range(count):
+                        ready.acquire()
+                        lab, res = srv.wait(tickets[i], timeout=600.0)
+                        done_at[i] = time.perf_counter()
+                        lat.append(res.time_ms)
+                        queued.append(res.plan_ms)
+                        labels.setdefault(int(picks[i]), lab)
+
+                th = threading.Thread(target=waiter)
+                th.start()
+                start = time.perf_counter()
+                for i in range(count):
+                    due = start + arrivals[i]
+                    while True:
+                        d = due - time.perf_counter()
+                        if d <= 0:
+                            break
+                        if d > 0.002:
+                            time.sleep(d - 0.001)
+                    k = int(picks[i])
+                    tickets[i] = (srv.submit_device(arena[k][1], arena[k][0]) if arm == "arena"
+                                  else srv.submit(graphs[k]))
+                    ready.release()
+                th.join()
+                span = max(done_at) - start
+                st = srv.stats()
+                srv.close()
+                served = quality({k: ctx.modularity(graphs[k], lab) for k, lab in labels.items()})
+                edges = int(sum(graphs[int(k)].m for k in picks))
+                arms[f"{arm}_{rate}"] = {
+                    "arm": arm, "rate_req_s": rate, "requests": count, "large_requests": int(np.sum(picks == len(pool))),
+                    "graphs_per_s": count / span, "edges_per_s": edges / span, "offered_s": float(arrivals[-1]),
+                    "span_s": span, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                    "queue_p50_ms": float(np.percentile(queued, 50)), "queue_p99_ms": float(np.percentile(queued, 99)),
+                    "launches": int(st["launches"]), "graphs_per_launch": count / max(1, st["launches"]),
+                    "max_concurrent_launches": int(st["max_concurrent_launches"]),
+                    "load_ms_per_launch": st["load_ms"] / max(1, st["launches"]),
+                    "run_ms_per_launch": st["run_ms"] / max(1, st["launches"]),
+                    "modularity": served}
+                log(f"[serving] {arm} {rate} req/s: {arms[f'{arm}_{rate}']}")
+    finally:
+        for a in registered:
+            cudart.cudaHostUnregister(a.ctypes.data)
+    return {"pool": "64 graphs of the batched-launch mix (seed %d) + 1 symmetric R-MAT scale 22 ef 16" % seed,
+            "modularity_control": dict(control, what="each graph alone, run twice (async LPA's own spread)"),
+            "mix": "98%% pool (uniform), 2%% scale-22; Poisson arrivals for %.1f s per rate" % seconds,
+            "server": "rak_server, 2 slots, <=256 graphs per launch, 16 GB budget, async mode, validate off "
+                      "(pool validated once)", "arms": arms}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -333,6 +443,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-graphs", type=int, default=256,
                     help="graphs in the batched-launch comparison (4096 = the full mix; 0 = skip)")
+    ap.add_argument("--serving-seconds", type=float, default=2.0,
+                    help="seconds of Poisson arrivals per rate in the serving comparison (0 = skip)")
+    ap.add_argument("--serving-rates", default="200,1000,5000")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -465,6 +578,9 @@ def main():
     batched = None
     if args.batch_graphs > 0:
         batched = batched_leg(ctx, args.batch_graphs, 3, threads, stream)
+    serving = None
+    if args.serving_seconds > 0 and world == 1:
+        serving = serving_leg(ctx, [int(x) for x in args.serving_rates.split(",")], args.serving_seconds, threads)
 
     if rank == 0:
         last = results[-1]
@@ -476,7 +592,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
-                "gpu_launches": 3 * args.steps, "batched": batched,
+                "gpu_launches": 3 * args.steps, "batched": batched, "serving": serving,
                 "run": {"iterations": last.iterations, "traversed_edges_per_step": last.traversed_edges,
                         "processed_vertices_per_step": last.processed_vertices,
                         "moved_vertices_per_step": last.moved_vertices, "loop_ms": last.loop_ms,

@@ -227,13 +227,23 @@ typedef struct rak_server_stats {
   uint64_t device_bytes_in_use; /* budget currently held by admitted requests */
   int32_t max_concurrent_launches;
   int32_t pending;              /* requests waiting for admission */
+  double load_ms;               /* host time packing and uploading launches, plan included (summed) */
+  double plan_ms;               /* of which building the plan on the device (summed) */
+  double run_ms;                /* launch-to-completion time of launches (summed) */
+  double pack_ms;               /* of load_ms: enqueueing uploads and the gather, checks included */
+  double plan_host_ms;          /* of load_ms: building the plan, waits included */
+  double enqueue_ms;            /* host time enqueueing the persistent launches (summed) */
 } rak_server_stats;
 
 void rak_server_options_default(rak_server_options *o);
 /* Starts the loop on ctx's device. */
 rak_status rak_server_create(rak_ctx *ctx, const rak_server_options *o, rak_server **out);
-/* Queues a host-located graph; its arrays must stay valid and unchanged until the request
- * completes (page-locked arrays copy fastest). RAK_ERR_BUSY when the queue is full. */
+/* Queues a graph; its arrays must stay valid and unchanged until the request completes.
+ * Host-located graphs are uploaded when their launch is packed (page-locked arrays copy fastest)
+ * and, with run.validate, checked here on the caller's thread. Device-located graphs (on the
+ * server's device: an arena of graphs kept in HBM) are packed by a device-to-device gather and,
+ * with run.validate, checked on the device before their launch; a graph that fails ends with
+ * RAK_ERR_INVALID_CSR from rak_server_wait. RAK_ERR_BUSY when the queue is full. */
 rak_status rak_server_submit(rak_server *s, const rak_csr *g, uint64_t *ticket);
 /* Waits up to timeout_s for a request (RAK_ERR_TIMEOUT otherwise), then copies its membership
  * (host, n entries; may be NULL) and result: iterations; time_ms = latency from submit to

@@ -44,25 +44,59 @@ struct Tracker {
   void sub(uint64_t b) { cur -= std::min(cur, b); }
 };
 
+// Where this thread's device allocations come from: cudaMalloc (no pool), or stream-ordered from
+// a memory pool on a stream (PoolScope). The server's launch slots use their own pools, so that
+// growing a slot's buffers never waits for the whole device (cudaFree does).
+struct PoolTarget {
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t stream = nullptr;
+};
+inline PoolTarget &thread_pool() {
+  static thread_local PoolTarget t;
+  return t;
+}
+struct PoolScope {
+  PoolTarget saved;
+  PoolScope(cudaMemPool_t pool, cudaStream_t stream) : saved(thread_pool()) { thread_pool() = {pool, stream}; }
+  ~PoolScope() { thread_pool() = saved; }
+};
+
+// Allocates from the current PoolScope's pool, else with cudaMalloc.
+inline cudaError_t dev_alloc(void **p, size_t bytes, cudaStream_t *freed_on) {
+  const PoolTarget &pt = thread_pool();
+  *freed_on = pt.stream;
+  if (pt.pool) return cudaMallocFromPoolAsync(p, bytes, pt.pool, pt.stream);
+  return cudaMalloc(p, bytes);
+}
+inline void dev_free(void *p, bool pooled, cudaStream_t freed_on) {
+  if (!p) return;
+  if (pooled) cudaFreeAsync(p, freed_on);
+  else cudaFree(p);
+}
+
 struct DevBuf {
   void *p = nullptr;
   size_t bytes = 0;
   Tracker *t = nullptr;
+  bool pooled = false;
+  cudaStream_t fs = nullptr;  // stream a pooled buffer is freed on
   DevBuf() = default;
   DevBuf(const DevBuf &) = delete;
   DevBuf &operator=(const DevBuf &) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (p) { cudaFree(p); if (t) t->sub(bytes); }
+    if (p) { dev_free(p, pooled, fs); if (t) t->sub(bytes); }
     p = nullptr;
     bytes = 0;
+    pooled = false;
   }
   cudaError_t alloc(size_t b, Tracker *tr) {
     release();
     bytes = b ? b : 16;
     t = tr;
-    cudaError_t e = cudaMalloc(&p, bytes);
-    if (e != cudaSuccess) { p = nullptr; bytes = 0; return e; }
+    pooled = thread_pool().pool != nullptr;
+    cudaError_t e = dev_alloc(&p, bytes, &fs);
+    if (e != cudaSuccess) { p = nullptr; bytes = 0; pooled = false; return e; }
     if (t) t->add(bytes);
     return e;
   }
@@ -99,6 +133,8 @@ struct rak_graph {
   float plan_ms = 0, h2d_ms = 0;
   size_t off_cap = 0, tgt_cap = 0, wt_cap = 0;  // bytes allocated for an owned copy
   void *wt_alloc = nullptr;                      // owned weight buffer (wt may be null: unit weights)
+  bool arrays_pooled = false;                    // owned arrays come from a server slot's pool
+  cudaStream_t arrays_fs = nullptr;              // ... and are freed on this stream
   rak_host_detail::RunBufs bufs;  // run buffers reused across runs
   // plan storage (order and split-vertex tables) and its build space, grown only when too small
   rak_host_detail::DevBuf p_order, p_hub_first, p_chunk_hub, p_keys, p_keys2, p_vids, p_hist, p_temp, p_deg;
@@ -124,9 +160,11 @@ using rak_host_detail::RunBufs;
 using rak_host_detail::Tracker;
 
 // Reuses a cached buffer when it is large enough (untracked: it outlives the call).
+// Grows d to at least `bytes` (contents are not kept). A buffer that has to grow again gets half
+// as much again, so a series of slightly larger requests does not reallocate every time.
 cudaError_t ensure(DevBuf &d, size_t bytes) {
   if (d.p && d.bytes >= bytes) return cudaSuccess;
-  return d.alloc(bytes, nullptr);
+  return d.alloc(d.p ? bytes + bytes / 2 : bytes, nullptr);
 }
 
 void set_err(rak_ctx *ctx, const char *fmt, ...) {
@@ -226,14 +264,30 @@ rak_status check_csr_shape(rak_ctx *ctx, const rak_csr *g) {
   return RAK_OK;
 }
 
+// Branch-free inside blocks of 64K entries so that the scans vectorise; the target scan of a
+// large graph is split over OpenMP threads.
 template <class O>
 rak_status validate_host_t(const O *off, const uint32_t *tgt, int64_t n, int64_t m) {
   if (int64_t(off[0]) != 0 || int64_t(off[n]) != m) return RAK_ERR_INVALID_CSR;
-  for (int64_t u = 0; u < n; ++u)
-    if (off[u] > off[u + 1]) return RAK_ERR_INVALID_CSR;
-  for (int64_t e = 0; e < m; ++e)
-    if (int64_t(tgt[e]) >= n) return RAK_ERR_INVALID_CSR;
-  return RAK_OK;
+  constexpr int64_t BLK = 1 << 16;
+  for (int64_t b = 0; b < n; b += BLK) {
+    const int64_t e = std::min(n, b + BLK);
+    unsigned bad = 0;
+    for (int64_t u = b; u < e; ++u) bad |= unsigned(off[u] > off[u + 1]);
+    if (bad) return RAK_ERR_INVALID_CSR;
+  }
+  if (n >= (int64_t(1) << 32)) return RAK_OK;  // every 32-bit target is in range
+  const uint32_t lim = uint32_t(n);
+  const int64_t nblk = (m + BLK - 1) / BLK;
+  unsigned bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad) if (m >= (int64_t(1) << 21))
+  for (int64_t k = 0; k < nblk; ++k) {
+    const int64_t b = k * BLK, e = std::min(m, b + BLK);
+    unsigned blk = 0;
+    for (int64_t i = b; i < e; ++i) blk |= unsigned(tgt[i] >= lim);
+    bad |= blk;
+  }
+  return bad ? RAK_ERR_INVALID_CSR : RAK_OK;
 }
 
 int nkeys_of(const Layout &ly) { return int(6 + ly.lane_max + 1); }
@@ -577,9 +631,9 @@ rak_status rak_graph_destroy(rak_graph *gr) {
   if (!gr) return RAK_ERR_INVALID_ARGUMENT;
   cudaSetDevice(gr->device);
   if (gr->owns) {
-    cudaFree(const_cast<void *>(gr->off));
-    cudaFree(const_cast<uint32_t *>(gr->tgt));
-    cudaFree(gr->wt_alloc);
+    rak_host_detail::dev_free(const_cast<void *>(gr->off), gr->arrays_pooled, gr->arrays_fs);
+    rak_host_detail::dev_free(const_cast<uint32_t *>(gr->tgt), gr->arrays_pooled, gr->arrays_fs);
+    rak_host_detail::dev_free(gr->wt_alloc, gr->arrays_pooled, gr->arrays_fs);
   }
   delete gr;
   return RAK_OK;
@@ -898,7 +952,7 @@ rak_status rak_batch_create(rak_ctx *ctx, const rak_batch_csr *bc, const rak_opt
   RAK_TRY(ctx, cudaMemcpyAsync(b->vbase.p, bc->graph_offsets, gbytes,
                                bc->location == RAK_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, ctx->stream));
   RAK_TRY(ctx, b->gid.alloc(size_t(std::max<int64_t>(bc->n, 1)) * 4, nullptr));
-  RAK_TRY(ctx, rak::launch_batch_gid(b->vbase.as<int64_t>(), bc->graphs, b->gid.as<uint32_t>(), ctx->stream));
+  RAK_TRY(ctx, rak::launch_batch_gid(b->vbase.as<int64_t>(), bc->graphs, bc->n, b->gid.as<uint32_t>(), ctx->stream));
   if (r.validate && bc->location == RAK_DEVICE) {
     DevBuf bad;
     unsigned int hbad = 0;
@@ -1036,7 +1090,7 @@ using Clock = std::chrono::steady_clock;
 
 struct ServerRequest {
   uint64_t ticket = 0;
-  rak_csr g{};        // the caller's host arrays (valid until completion)
+  rak_csr g{};        // the caller's arrays, host or device (valid until completion)
   uint64_t bytes = 0; // budget held while admitted
   Clock::time_point t_submit, t_launch, t_done;
   std::vector<uint32_t> membership;
@@ -1059,7 +1113,7 @@ struct Pinned {
     if (p) cudaFreeHost(p);
     p = nullptr;
     bytes = 0;
-    const size_t want = b + b / 2 + 4096;
+    const size_t want = std::max<size_t>(b + b / 2 + 4096, size_t(1) << 20);
     cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
     if (e == cudaSuccess) bytes = want;
     else p = nullptr;
@@ -1072,11 +1126,13 @@ struct Pinned {
 struct ServerSlot {
   rak_ctx *ctx = nullptr;
   rak_batch *b = nullptr;
-  Pinned h_go, h_off, h_mem, h_it;
-  DevBuf d_mem;
+  Pinned h_go, h_mem, h_it, h_bad;
+  DevBuf d_mem, d_items, d_bad, d_stage;
+  cudaMemPool_t pool = nullptr;  // stream-ordered device allocations of this slot
   cudaEvent_t ev = nullptr;
   std::vector<ReqPtr> reqs;
   std::vector<int64_t> vo;
+  Clock::time_point t_launch;
   bool busy = false;       // holds requests
   bool launching = false;  // requests taken, event not recorded yet
 };
@@ -1087,16 +1143,18 @@ uint64_t request_bytes(const rak_csr &g) {
   return 8 * (n + 1) + 4 * m + (g.weights ? 4 * m : 0) + 32 * n + 256;
 }
 
-// Grows an owned device array of a graph (contents are not kept).
-cudaError_t grow(const void *&p, size_t &cap, size_t need) {
+// Grows an owned device array of a slot's batch graph (contents are not kept), stream-ordered
+// from the slot's pool (the caller holds a PoolScope).
+cudaError_t grow(rak_graph *gr, const void *&p, size_t &cap, size_t need) {
   if (p && cap >= need) return cudaSuccess;
-  cudaFree(const_cast<void *>(p));
+  rak_host_detail::dev_free(const_cast<void *>(p), gr->arrays_pooled, gr->arrays_fs);
   p = nullptr;
   cap = 0;
   void *q = nullptr;
   const size_t want = need + need / 2 + 256;
-  cudaError_t e = cudaMalloc(&q, want);
+  cudaError_t e = rak_host_detail::dev_alloc(&q, want, &gr->arrays_fs);
   if (e != cudaSuccess) return e;
+  gr->arrays_pooled = rak_host_detail::thread_pool().pool != nullptr;
   p = q;
   cap = want;
   return cudaSuccess;
@@ -1123,102 +1181,176 @@ struct rak_server {
 
 namespace {
 
-// Packs the slot's requests into its batch on the device: offsets rebased on the host into
-// page-locked staging, targets and weights copied straight from the callers' arrays.
+// Fails the slot's requests whose flag in bad[] is set (graphs that break the CSR rules) and
+// drops them from the slot.
+void server_drop_invalid(rak_server *s, ServerSlot &sl, const unsigned int *bad) {
+  std::vector<ReqPtr> keep;
+  std::lock_guard<std::mutex> lk(s->mu);
+  const auto now = Clock::now();
+  for (size_t i = 0; i < sl.reqs.size(); ++i) {
+    if (!bad[i]) { keep.push_back(sl.reqs[i]); continue; }
+    ServerRequest &r = *sl.reqs[i];
+    r.status = RAK_ERR_INVALID_CSR;
+    r.done = true;
+    r.t_done = now;
+    s->used -= r.bytes;
+    s->st.rejected++;
+  }
+  sl.reqs = std::move(keep);
+  s->cv_done.notify_all();
+}
+
+// Packs the slot's requests into its batch on the device. Host-located graphs: targets and
+// weights uploaded straight into their place, offsets uploaded as they are into a staging area.
+// One gather kernel then rebases every graph's offsets and copies the edges of device-located
+// graphs, checking the CSR rules; with validation on, the flags are read back and failing graphs
+// are dropped before the plan is built (host graphs were checked at submission).
 rak_status server_load(rak_server *s, ServerSlot &sl) {
   rak_ctx *ctx = sl.ctx;
   cudaStream_t st = ctx->stream;
-  const size_t G = sl.reqs.size();
-  sl.vo.assign(G + 1, 0);
-  int64_t m_tot = 0;
-  bool weighted = false;
-  for (size_t i = 0; i < G; ++i) {
-    sl.vo[i + 1] = sl.vo[i] + sl.reqs[i]->g.n;
-    m_tot += sl.reqs[i]->g.m;
-    weighted |= sl.reqs[i]->g.weights != nullptr;
-  }
-  const int64_t n_tot = sl.vo[G];
-  RAK_TRY(ctx, sl.h_go.ensure((G + 1) * 8));
-  RAK_TRY(ctx, sl.h_off.ensure(size_t(n_tot + 1) * 8));
-  int64_t *go = sl.h_go.as<int64_t>(), *off = sl.h_off.as<int64_t>();
-  int64_t e_base = 0;
-  for (size_t i = 0; i < G; ++i) {
-    go[i] = sl.vo[i];
-    const rak_csr &g = sl.reqs[i]->g;
-    int64_t *o = off + sl.vo[i];
-    if (g.offset_bits == 64) {
-      const int64_t *src = static_cast<const int64_t *>(g.offsets);
-      for (int64_t u = 0; u < g.n; ++u) o[u] = src[u] + e_base;
-    } else {
-      const int32_t *src = static_cast<const int32_t *>(g.offsets);
-      for (int64_t u = 0; u < g.n; ++u) o[u] = int64_t(src[u]) + e_base;
+  const auto t0 = Clock::now();
+  for (;;) {
+    const size_t G = sl.reqs.size();
+    if (G == 0) return RAK_OK;
+    sl.vo.assign(G + 1, 0);
+    std::vector<int64_t> eo(G + 1, 0), so(G + 1, 0);  // first edge slot; staging byte offset
+    int64_t max_elems = 0;
+    bool weighted = false;
+    for (size_t i = 0; i < G; ++i) {
+      const rak_csr &g = sl.reqs[i]->g;
+      sl.vo[i + 1] = sl.vo[i] + g.n;
+      eo[i + 1] = eo[i] + g.m;
+      const int64_t ob = g.location == RAK_HOST ? ((g.n + 1) * (g.offset_bits / 8) + 15) / 16 * 16 : 0;
+      so[i + 1] = so[i] + ob;
+      weighted |= g.weights != nullptr;
+      max_elems = std::max(max_elems, std::max(g.n, g.location == RAK_DEVICE ? g.m : 0));
     }
-    e_base += g.m;
-  }
-  go[G] = n_tot;
-  off[n_tot] = m_tot;
-  if (!sl.b) {
-    auto *b = new (std::nothrow) rak_batch();
-    auto *gr = new (std::nothrow) rak_graph();
-    if (!b || !gr) { delete b; delete gr; return RAK_ERR_OUT_OF_MEMORY; }
-    gr->ctx = ctx;
-    gr->device = ctx->device;
-    gr->owns = true;
-    gr->off64 = true;
-    b->ctx = ctx;
-    b->device = ctx->device;
-    b->g = gr;
-    sl.b = b;
-  }
-  rak_batch *b = sl.b;
-  rak_graph *gr = b->g;
-  RAK_TRY(ctx, grow(gr->off, gr->off_cap, size_t(n_tot + 1) * 8));
-  const void *tp = gr->tgt;
-  RAK_TRY(ctx, grow(tp, gr->tgt_cap, size_t(std::max<int64_t>(m_tot, 1)) * 4));
-  gr->tgt = static_cast<const uint32_t *>(tp);
-  if (weighted) {
-    const void *wp = gr->wt_alloc;
-    RAK_TRY(ctx, grow(wp, gr->wt_cap, size_t(std::max<int64_t>(m_tot, 1)) * 4));
-    gr->wt_alloc = const_cast<void *>(wp);
-  }
-  gr->n = n_tot;
-  gr->m = m_tot;
-  gr->wt = weighted ? static_cast<const float *>(gr->wt_alloc) : nullptr;
-  gr->graph_bytes = gr->off_cap + gr->tgt_cap + gr->wt_cap;
-  RAK_TRY(ctx, cudaMemcpyAsync(const_cast<void *>(gr->off), off, size_t(n_tot + 1) * 8, cudaMemcpyHostToDevice, st));
-  e_base = 0;
-  for (size_t i = 0; i < G; ++i) {
-    const rak_csr &g = sl.reqs[i]->g;
-    if (g.m > 0) {
-      RAK_TRY(ctx, cudaMemcpyAsync(const_cast<uint32_t *>(gr->tgt) + e_base, g.targets, size_t(g.m) * 4,
+    const int64_t n_tot = sl.vo[G], m_tot = eo[G];
+    if (!sl.b) {
+      auto *b = new (std::nothrow) rak_batch();
+      auto *gr = new (std::nothrow) rak_graph();
+      if (!b || !gr) { delete b; delete gr; return RAK_ERR_OUT_OF_MEMORY; }
+      gr->ctx = ctx;
+      gr->device = ctx->device;
+      gr->owns = true;
+      gr->off64 = true;
+      b->ctx = ctx;
+      b->device = ctx->device;
+      b->g = gr;
+      sl.b = b;
+    }
+    rak_batch *b = sl.b;
+    rak_graph *gr = b->g;
+    RAK_TRY(ctx, grow(gr, gr->off, gr->off_cap, size_t(n_tot + 1) * 8));
+    const void *tp = gr->tgt;
+    RAK_TRY(ctx, grow(gr, tp, gr->tgt_cap, size_t(std::max<int64_t>(m_tot, 1)) * 4));
+    gr->tgt = static_cast<const uint32_t *>(tp);
+    if (weighted) {
+      const void *wp = gr->wt_alloc;
+      RAK_TRY(ctx, grow(gr, wp, gr->wt_cap, size_t(std::max<int64_t>(m_tot, 1)) * 4));
+      gr->wt_alloc = const_cast<void *>(wp);
+    }
+    gr->n = n_tot;
+    gr->m = m_tot;
+    gr->wt = weighted ? static_cast<const float *>(gr->wt_alloc) : nullptr;
+    gr->graph_bytes = gr->off_cap + gr->tgt_cap + gr->wt_cap;
+    int64_t *d_off = static_cast<int64_t *>(const_cast<void *>(gr->off));
+    uint32_t *d_tgt = const_cast<uint32_t *>(gr->tgt);
+    float *d_wt = weighted ? static_cast<float *>(gr->wt_alloc) : nullptr;
+    RAK_TRY(ctx, ensure(sl.d_stage, size_t(std::max<int64_t>(so[G], 16))));
+    char *stage = sl.d_stage.as<char>();
+    // pinned: graph vertex offsets (G + 1), the final edge offset, then the gather items
+    RAK_TRY(ctx, sl.h_go.ensure((G + 2) * 8 + G * sizeof(rak::GatherItem) + 64));
+    int64_t *go = sl.h_go.as<int64_t>();
+    auto *items = reinterpret_cast<rak::GatherItem *>(go + G + 2);
+    for (size_t i = 0; i <= G; ++i) go[i] = sl.vo[i];
+    go[G + 1] = m_tot;
+    for (size_t i = 0; i < G; ++i) {
+      const rak_csr &g = sl.reqs[i]->g;
+      rak::GatherItem &it = items[i];
+      it.n = g.n;
+      it.m = g.m;
+      it.vdst = sl.vo[i];
+      it.edst = eo[i];
+      it.off64 = g.offset_bits == 64;
+      it.pad = 0;
+      if (g.location == RAK_DEVICE) {
+        it.off = g.offsets;
+        it.tgt = g.targets;
+        it.wt = g.weights;
+        continue;
+      }
+      it.off = stage + so[i];
+      it.tgt = nullptr;
+      it.wt = nullptr;
+      RAK_TRY(ctx, cudaMemcpyAsync(stage + so[i], g.offsets, size_t(g.n + 1) * (g.offset_bits / 8),
                                    cudaMemcpyHostToDevice, st));
-      float *w = static_cast<float *>(gr->wt_alloc) + e_base;
-      if (weighted && g.weights) RAK_TRY(ctx, cudaMemcpyAsync(w, g.weights, size_t(g.m) * 4, cudaMemcpyHostToDevice, st));
-      else if (weighted) RAK_TRY(ctx, rak::launch_fill_f32(w, g.m, 1.0f, st));
+      if (g.m > 0) {
+        RAK_TRY(ctx, cudaMemcpyAsync(d_tgt + eo[i], g.targets, size_t(g.m) * 4, cudaMemcpyHostToDevice, st));
+        if (weighted && g.weights)
+          RAK_TRY(ctx, cudaMemcpyAsync(d_wt + eo[i], g.weights, size_t(g.m) * 4, cudaMemcpyHostToDevice, st));
+        else if (weighted) RAK_TRY(ctx, rak::launch_fill_f32(d_wt + eo[i], g.m, 1.0f, st));
+      }
     }
-    e_base += g.m;
+    RAK_TRY(ctx, ensure(sl.d_items, G * sizeof(rak::GatherItem)));
+    RAK_TRY(ctx, ensure(sl.d_bad, G * 4));
+    RAK_TRY(ctx, cudaMemcpyAsync(sl.d_items.p, items, G * sizeof(rak::GatherItem), cudaMemcpyHostToDevice, st));
+    RAK_TRY(ctx, cudaMemcpyAsync(d_off + n_tot, go + G + 1, 8, cudaMemcpyHostToDevice, st));
+    RAK_TRY(ctx, cudaMemsetAsync(sl.d_bad.p, 0, G * 4, st));
+    RAK_TRY(ctx, rak::launch_gather_graphs(sl.d_items.as<rak::GatherItem>(), int(G), max_elems, d_off, d_tgt, d_wt,
+                                           sl.d_bad.as<unsigned int>(), st));
+    if (s->run.validate) {
+      RAK_TRY(ctx, sl.h_bad.ensure(G * 4));
+      RAK_TRY(ctx, cudaMemcpyAsync(sl.h_bad.p, sl.d_bad.p, G * 4, cudaMemcpyDeviceToHost, st));
+      RAK_TRY(ctx, cudaStreamSynchronize(st));
+      const unsigned int *bad = sl.h_bad.as<unsigned int>();
+      bool any = false;
+      for (size_t i = 0; i < G; ++i) any |= bad[i] != 0;
+      if (any) {
+        server_drop_invalid(s, sl, bad);
+        continue;  // pack the remaining requests again
+      }
+    }
+    b->ngraphs = int64_t(G);
+    RAK_TRY(ctx, ensure(b->vbase, (G + 1) * 8));
+    RAK_TRY(ctx, cudaMemcpyAsync(b->vbase.p, go, (G + 1) * 8, cudaMemcpyHostToDevice, st));
+    RAK_TRY(ctx, ensure(b->gid, size_t(std::max<int64_t>(n_tot, 1)) * 4));
+    RAK_TRY(ctx, rak::launch_batch_gid(b->vbase.as<int64_t>(), int64_t(G), n_tot, b->gid.as<uint32_t>(), st));
+    const auto t1 = Clock::now();
+    const rak_status ps = build_plan(ctx, gr, s->run.ly, nullptr);
+    const auto t2 = Clock::now();
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->st.pack_ms += std::chrono::duration<double, std::milli>(t1 - t0).count();
+    s->st.plan_host_ms += std::chrono::duration<double, std::milli>(t2 - t1).count();
+    return ps;
   }
-  b->ngraphs = int64_t(G);
-  RAK_TRY(ctx, ensure(b->vbase, (G + 1) * 8));
-  RAK_TRY(ctx, cudaMemcpyAsync(b->vbase.p, go, (G + 1) * 8, cudaMemcpyHostToDevice, st));
-  RAK_TRY(ctx, ensure(b->gid, size_t(std::max<int64_t>(n_tot, 1)) * 4));
-  RAK_TRY(ctx, rak::launch_batch_gid(b->vbase.as<int64_t>(), int64_t(G), b->gid.as<uint32_t>(), st));
-  return build_plan(ctx, gr, s->run.ly, nullptr);
 }
 
 rak_status server_launch(rak_server *s, ServerSlot &sl) {
+  rak_host_detail::PoolScope scope(sl.pool, sl.ctx->stream);
+  const auto t0 = Clock::now();
   RAK_CHECK(server_load(s, sl));
+  if (sl.reqs.empty()) return RAK_OK;  // every request failed its check
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->st.load_ms += std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+    s->st.plan_ms += sl.b->g->plan_ms;
+  }
+  sl.t_launch = Clock::now();
   rak_ctx *ctx = sl.ctx;
   rak_batch *b = sl.b;
   const int64_t n = b->g->n, G = b->ngraphs;
   RAK_CHECK(batch_prepare(ctx, b, s->run));
   RAK_TRY(ctx, ensure(sl.d_mem, size_t(std::max<int64_t>(n, 1)) * 4));
+  const auto t_prepared = Clock::now();
   RAK_TRY(ctx, sl.h_mem.ensure(size_t(std::max<int64_t>(n, 1)) * 4));
   RAK_TRY(ctx, sl.h_it.ensure(size_t(std::max<int64_t>(G, 1)) * 4));
   RAK_CHECK(batch_enqueue(ctx, b, nullptr, s->run, sl.d_mem.as<uint32_t>(), s->grid_cap));
   RAK_TRY(ctx, cudaMemcpyAsync(sl.h_mem.p, sl.d_mem.p, size_t(n) * 4, cudaMemcpyDeviceToHost, ctx->stream));
   RAK_TRY(ctx, cudaMemcpyAsync(sl.h_it.p, b->giters.p, size_t(G) * 4, cudaMemcpyDeviceToHost, ctx->stream));
   RAK_TRY(ctx, cudaEventRecord(sl.ev, ctx->stream));
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->st.enqueue_ms += std::chrono::duration<double, std::milli>(Clock::now() - t_prepared).count();
   return RAK_OK;
 }
 
@@ -1244,6 +1376,7 @@ void server_loop(rak_server *s) {
         s->st.completed++;
         s->st.edges_completed += uint64_t(r.g.m);
       }
+      s->st.run_ms += std::chrono::duration<double, std::milli>(now - sl.t_launch).count();
       sl.reqs.clear();
       sl.busy = false;
       s->cv_done.notify_all();
@@ -1284,6 +1417,7 @@ void server_loop(rak_server *s) {
         const rak_status rs = server_launch(s, *free_slot);
         lk.lock();
         free_slot->launching = false;
+        if (rs == RAK_OK && free_slot->reqs.empty()) free_slot->busy = false;
         if (rs != RAK_OK) {
           for (auto &r : free_slot->reqs) {
             r->status = rs;
@@ -1340,8 +1474,24 @@ rak_status rak_server_create(rak_ctx *ctx, const rak_server_options *o, rak_serv
     ServerSlot &sl = *s->slots.back();
     st = rak_ctx_create(ctx->device, &sl.ctx);
     if (st == RAK_OK && cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) != cudaSuccess) st = RAK_ERR_CUDA;
+    if (st == RAK_OK) {
+      // the slot's own pool keeps what it has allocated (release threshold: everything), so a
+      // slot's buffers, once grown, are reused without going back to the driver
+      cudaMemPoolProps props{};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = ctx->device;
+      uint64_t keep = ~uint64_t(0);
+      if (cudaMemPoolCreate(&sl.pool, &props) != cudaSuccess ||
+          cudaMemPoolSetAttribute(sl.pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess)
+        st = RAK_ERR_CUDA;
+    }
     if (st != RAK_OK) {
-      for (auto &x : s->slots) { if (x->ev) cudaEventDestroy(x->ev); if (x->ctx) rak_ctx_destroy(x->ctx); }
+      for (auto &x : s->slots) {
+        if (x->pool) cudaMemPoolDestroy(x->pool);
+        if (x->ev) cudaEventDestroy(x->ev);
+        if (x->ctx) rak_ctx_destroy(x->ctx);
+      }
       delete s;
       return st;
     }
@@ -1353,8 +1503,10 @@ rak_status rak_server_create(rak_ctx *ctx, const rak_server_options *o, rak_serv
 
 rak_status rak_server_submit(rak_server *s, const rak_csr *g, uint64_t *ticket) {
   if (!s || !g || !ticket) return RAK_ERR_INVALID_ARGUMENT;
-  if (check_csr_shape(nullptr, g) != RAK_OK || g->location != RAK_HOST) return RAK_ERR_INVALID_ARGUMENT;
-  if (s->run.validate && rak_csr_validate_host(g) != RAK_OK) return RAK_ERR_INVALID_CSR;
+  if (check_csr_shape(nullptr, g) != RAK_OK || (g->location != RAK_HOST && g->location != RAK_DEVICE))
+    return RAK_ERR_INVALID_ARGUMENT;
+  // host graphs are checked here, on the caller's thread; device graphs when their launch is packed
+  if (g->location == RAK_HOST && s->run.validate && rak_csr_validate_host(g) != RAK_OK) return RAK_ERR_INVALID_CSR;
   auto r = std::make_shared<ServerRequest>();
   r->g = *g;
   r->bytes = request_bytes(*g);
@@ -1417,8 +1569,11 @@ rak_status rak_server_destroy(rak_server *s) {
   for (auto &slp : s->slots) {
     ServerSlot &sl = *slp;
     if (sl.ctx) cudaStreamSynchronize(sl.ctx->stream);
-    if (sl.b) rak_batch_destroy(sl.b);
-    sl.d_mem.release();
+    if (sl.b) rak_batch_destroy(sl.b);  // pooled buffers are freed on the slot's stream
+    sl.b = nullptr;
+    for (DevBuf *d : {&sl.d_mem, &sl.d_items, &sl.d_bad, &sl.d_stage}) d->release();
+    if (sl.ctx) cudaStreamSynchronize(sl.ctx->stream);
+    if (sl.pool) cudaMemPoolDestroy(sl.pool);
     if (sl.ev) cudaEventDestroy(sl.ev);
     if (sl.ctx) rak_ctx_destroy(sl.ctx);
   }

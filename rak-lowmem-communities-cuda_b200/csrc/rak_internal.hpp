@@ -125,7 +125,18 @@ cudaError_t launch_modularity(const void *off, bool off64, const uint32_t *tgt, 
 
 // Batches of graphs (rak_kernels.cu).
 cudaError_t launch_fill_f32(float *p, int64_t count, float v, cudaStream_t st);
-cudaError_t launch_batch_gid(const int64_t *vbase, int64_t ngraphs, uint32_t *gid, cudaStream_t st);
+// One graph to pack into a batch CSR from device memory (k_gather_graphs).
+struct GatherItem {
+  const void *off;       // n + 1 offsets, int64 if off64 else int32
+  const uint32_t *tgt;   // m targets (graph-local ids); null: edges already in place
+  const float *wt;       // m weights, or null (unit)
+  int64_t n, m;
+  int64_t vdst, edst;    // first vertex and first edge slot in the batch
+  int32_t off64, pad;
+};
+cudaError_t launch_gather_graphs(const GatherItem *items, int count, int64_t max_elems, int64_t *off_dst,
+                                 uint32_t *tgt_dst, float *wt_dst, unsigned int *bad, cudaStream_t st);
+cudaError_t launch_batch_gid(const int64_t *vbase, int64_t ngraphs, int64_t n, uint32_t *gid, cudaStream_t st);
 cudaError_t launch_batch_validate(const int64_t *vbase, int64_t ngraphs, int64_t n, const int64_t *off,
                                   const uint32_t *tgt, const uint32_t *gid, unsigned int *bad, cudaStream_t st);
 cudaError_t launch_batch_init(uint32_t *v0, uint32_t *v1, const uint32_t *q, const uint32_t *gid,

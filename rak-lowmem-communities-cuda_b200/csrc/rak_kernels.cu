@@ -132,10 +132,17 @@ __global__ void k_mod_square(const double *ctot, int64_t n, double *sums) {
 
 // ---- batches of graphs ------------------------------------------------------------------------
 // gid[u] = graph of vertex u, from the graph vertex offsets.
-__global__ void k_batch_gid(const int64_t *vbase, int64_t ngraphs, uint32_t *gid) {
+__global__ void k_batch_gid(const int64_t *vbase, int64_t ngraphs, int64_t n, uint32_t *gid) {
   const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
-  for (int64_t g = tid; g < ngraphs; g += nt)
-    for (int64_t u = vbase[g]; u < vbase[g + 1]; ++u) gid[u] = uint32_t(g);
+  for (int64_t u = tid; u < n; u += nt) {  // the last g with vbase[g] <= u: binary search
+    int64_t lo = 0, hi = ngraphs;          // vbase[lo] <= u < vbase[hi]
+    while (hi - lo > 1) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (vbase[mid] <= u) lo = mid;
+      else hi = mid;
+    }
+    gid[u] = uint32_t(lo);
+  }
 }
 
 // Batch CSR rules: graph offsets non-decreasing from 0 to n, and every target (a local id) below
@@ -216,6 +223,39 @@ __global__ void k_fill_f32(float *p, int64_t count, float v) {
   for (int64_t i = tid; i < count; i += nt) p[i] = v;
 }
 
+// Packs graphs into a batch CSR: graph blockIdx.y's offsets rebased by its first edge slot, its
+// targets copied, its weights copied (or 1.0 where the batch is weighted and the graph is not);
+// an item without targets has its edges in place already (only the offsets are rebased). The CSR
+// rules are checked on the way (bad[y]: 1 = offsets, 2 = a target out of range); the copies touch
+// only the n + 1 offsets and m edges the graph declares.
+__global__ void k_gather_graphs(const GatherItem *items, int64_t *off_dst, uint32_t *tgt_dst, float *wt_dst,
+                                unsigned int *bad) {
+  const GatherItem it = items[blockIdx.y];
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  unsigned int b = 0;
+  const int64_t *o64 = static_cast<const int64_t *>(it.off);
+  const int32_t *o32 = static_cast<const int32_t *>(it.off);
+  for (int64_t u = tid; u < it.n; u += nt) {
+    const int64_t a = it.off64 ? o64[u] : int64_t(o32[u]);
+    const int64_t z = it.off64 ? o64[u + 1] : int64_t(o32[u + 1]);
+    off_dst[it.vdst + u] = a + it.edst;
+    if (a > z) b |= 1u;
+  }
+  if (tid == 0) {
+    const int64_t a = it.off64 ? o64[0] : int64_t(o32[0]);
+    const int64_t z = it.off64 ? o64[it.n] : int64_t(o32[it.n]);
+    if (a != 0 || z != it.m) b |= 1u;
+  }
+  const uint64_t lim = uint64_t(it.n);
+  for (int64_t e = tid; it.tgt && e < it.m; e += nt) {
+    const uint32_t t = it.tgt[e];
+    tgt_dst[it.edst + e] = t;
+    if (uint64_t(t) >= lim) b |= 2u;
+    if (wt_dst) wt_dst[it.edst + e] = it.wt ? it.wt[e] : 1.0f;
+  }
+  if (b) atomicOr(bad + blockIdx.y, b);
+}
+
 }  // namespace
 
 cudaError_t launch_fill_f32(float *p, int64_t count, float v, cudaStream_t st) {
@@ -223,8 +263,18 @@ cudaError_t launch_fill_f32(float *p, int64_t count, float v, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_batch_gid(const int64_t *vbase, int64_t ngraphs, uint32_t *gid, cudaStream_t st) {
-  k_batch_gid<<<grid_for(ngraphs), TPB, 0, st>>>(vbase, ngraphs, gid);
+cudaError_t launch_gather_graphs(const GatherItem *items, int count, int64_t max_elems, int64_t *off_dst,
+                                 uint32_t *tgt_dst, float *wt_dst, unsigned int *bad, cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  if (count > 65535) return cudaErrorInvalidValue;
+  const int64_t bx = (max_elems + int64_t(TPB) * 8 - 1) / (int64_t(TPB) * 8);
+  const dim3 grid(unsigned(bx < 1 ? 1 : (bx > 1024 ? 1024 : bx)), unsigned(count));
+  k_gather_graphs<<<grid, TPB, 0, st>>>(items, off_dst, tgt_dst, wt_dst, bad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_gid(const int64_t *vbase, int64_t ngraphs, int64_t n, uint32_t *gid, cudaStream_t st) {
+  k_batch_gid<<<grid_for(n, 4), TPB, 0, st>>>(vbase, ngraphs, n, gid);
   return cudaGetLastError();
 }
 

@@ -70,7 +70,8 @@ class rak_server_stats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("rejected", C.c_uint64),
                 ("launches", C.c_uint64), ("graphs_launched", C.c_uint64), ("edges_completed", C.c_uint64),
                 ("device_bytes_in_use", C.c_uint64), ("max_concurrent_launches", C.c_int32),
-                ("pending", C.c_int32)]
+                ("pending", C.c_int32), ("load_ms", C.c_double), ("plan_ms", C.c_double), ("run_ms", C.c_double),
+                ("pack_ms", C.c_double), ("plan_host_ms", C.c_double), ("enqueue_ms", C.c_double)]
 
 
 class rak_host_csr(C.Structure):
@@ -496,9 +497,15 @@ class Batch:
         return q[:self.graphs]
 
 
+class _DeviceRequest:
+    def __init__(self, n, keep):
+        self.n, self.keep = n, keep
+
+
 class Server:
-    """Continuous-batching request loop (rak_server_*). submit() takes host graphs, which must stay
-    alive and unchanged until wait() returns for them (the object keeps a reference)."""
+    """Continuous-batching request loop (rak_server_*). submit() takes host graphs and
+    submit_device() device-located graphs (a rak_csr from device_csr()); either must stay alive and
+    unchanged until wait() returns for it (the object keeps a reference to what it is given)."""
 
     def __init__(self, ctx: Context, budget_bytes=16 << 30, max_graphs_per_launch=256, slots=2,
                  queue_capacity=65536, **run_opts):
@@ -517,6 +524,14 @@ class Server:
         t = C.c_uint64(0)
         _check(_lib.rak_server_submit(self._s, C.byref(c), C.byref(t)))
         self._keep[t.value] = g
+        return t.value
+
+    def submit_device(self, csr, keep=None) -> int:
+        """Queues a device-located graph (rak_csr with location DEVICE, on the server's device);
+        `keep` is held until the request completes (the tensors behind the pointers)."""
+        t = C.c_uint64(0)
+        _check(_lib.rak_server_submit(self._s, C.byref(csr), C.byref(t)))
+        self._keep[t.value] = _DeviceRequest(int(csr.n), keep)
         return t.value
 
     def wait(self, ticket: int, timeout=120.0):

@@ -107,3 +107,60 @@ def test_full_queue_is_busy(ctx):
     for t in tickets:
         srv.wait(t)
     srv.close()
+
+
+def device_graph(g):
+    import torch
+    off = torch.from_numpy(np.ascontiguousarray(g.offsets)).cuda()
+    tgt = torch.from_numpy(g.targets.view(np.int32)).cuda()
+    wt = torch.from_numpy(g.weights).cuda() if g.weights is not None else None
+    return (off, tgt, wt), rl.device_csr(off, tgt, wt)
+
+
+def test_device_requests_same_as_host_requests(ctx):
+    """Graphs kept in device memory (an arena) are packed by the gather kernel; their results
+    equal those of the same graphs submitted from the host, and of each graph alone."""
+    gs = request_graphs()
+    alone = [ctx.lowmem(g, mode=rl.MODE_SYNC, **LAYOUT) for g in gs]
+    arena = [device_graph(g) for g in gs]
+    srv = rl.Server(ctx, max_graphs_per_launch=4, slots=2, mode=rl.MODE_SYNC, **LAYOUT)
+    ts = []
+    for i, g in enumerate(gs):          # host and device requests interleaved in the same launches
+        keep, csr = arena[i]
+        ts.append(srv.submit_device(csr, keep) if i % 3 else srv.submit(g))
+    for i, t in enumerate(ts):
+        lab, res = srv.wait(t)
+        np.testing.assert_array_equal(lab, alone[i][0], err_msg=f"request {i}")
+        assert res.iterations == alone[i][1].iterations
+    st = srv.stats()
+    assert st["completed"] == len(gs) and st["rejected"] == 0 and st["device_bytes_in_use"] == 0
+    srv.close()
+
+
+def test_invalid_device_graph_fails_others_served(ctx):
+    import torch
+    good = [rl.gen_rmat(9, 6, seed=40 + i) for i in range(3)]
+    alone = [ctx.lowmem(g, mode=rl.MODE_SYNC, **LAYOUT)[0] for g in good]
+    bad_tgt = good[0].targets.copy()
+    bad_tgt[len(bad_tgt) // 2] = good[0].n          # one target out of range
+    bad_off = good[1].offsets.copy()
+    bad_off[5], bad_off[6] = bad_off[6], bad_off[5] - 1   # offsets decrease
+    bads = []
+    for off, tgt in ((good[0].offsets, bad_tgt), (bad_off, good[1].targets)):
+        o = torch.from_numpy(np.ascontiguousarray(off)).cuda()
+        t = torch.from_numpy(tgt.view(np.int32)).cuda()
+        bads.append(((o, t), rl.device_csr(o, t, None)))
+    srv = rl.Server(ctx, max_graphs_per_launch=8, slots=1, mode=rl.MODE_SYNC, **LAYOUT)
+    ts_bad = [srv.submit_device(csr, keep) for keep, csr in bads]
+    arena = [device_graph(g) for g in good]
+    ts_good = [srv.submit_device(csr, keep) for keep, csr in arena]
+    for t in ts_bad:
+        with pytest.raises(rl.RakError) as e:
+            srv.wait(t)
+        assert e.value.status == 2
+    for t, want in zip(ts_good, alone):
+        lab, _ = srv.wait(t)
+        np.testing.assert_array_equal(lab, want)
+    st = srv.stats()
+    assert st["rejected"] == 2 and st["completed"] == 3 and st["device_bytes_in_use"] == 0
+    srv.close()
