@@ -376,6 +376,13 @@ def serving_leg(ctx, rates, seconds, threads, seed=11):
                 arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
                 picks = np.where(rng.random(count) < 0.02, len(pool), rng.integers(0, len(pool), count))
                 srv = rl.Server(ctx, slots=2, validate=0)
+                # warm-up, untimed: grows the server's pools and loads its kernels (a few pool graphs
+                # and the large one, alone and together)
+                for ks in ([0, 1, 2, 3], [len(pool)], [4, len(pool), 5]):
+                    for t in [(srv.submit_device(arena[k][1], arena[k][0]) if arm == "arena"
+                               else srv.submit(graphs[k])) for k in ks]:
+                        srv.wait(t, timeout=600.0)
+                st0 = srv.stats()
                 tickets = [None] * count
                 lat, queued, done_at, labels = [], [], [0.0] * count, {}
                 ready = threading.Semaphore(0)
@@ -415,10 +422,11 @@ def serving_leg(ctx, rates, seconds, threads, seed=11):
                     "graphs_per_s": count / span, "edges_per_s": edges / span, "offered_s": float(arrivals[-1]),
                     "span_s": span, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                     "queue_p50_ms": float(np.percentile(queued, 50)), "queue_p99_ms": float(np.percentile(queued, 99)),
-                    "launches": int(st["launches"]), "graphs_per_launch": count / max(1, st["launches"]),
+                    "launches": int(st["launches"] - st0["launches"]),
+                    "graphs_per_launch": count / max(1, st["launches"] - st0["launches"]),
                     "max_concurrent_launches": int(st["max_concurrent_launches"]),
-                    "load_ms_per_launch": st["load_ms"] / max(1, st["launches"]),
-                    "run_ms_per_launch": st["run_ms"] / max(1, st["launches"]),
+                    "load_ms_per_launch": (st["load_ms"] - st0["load_ms"]) / max(1, st["launches"] - st0["launches"]),
+                    "run_ms_per_launch": (st["run_ms"] - st0["run_ms"]) / max(1, st["launches"] - st0["launches"]),
                     "modularity": served}
                 log(f"[serving] {arm} {rate} req/s: {arms[f'{arm}_{rate}']}")
     finally:
@@ -441,6 +449,7 @@ def main():
     ap.add_argument("--slots", type=int, default=8)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--batch-graphs", type=int, default=256,
                     help="graphs in the batched-launch comparison (4096 = the full mix; 0 = skip)")
     ap.add_argument("--serving-seconds", type=float, default=2.0,
@@ -533,6 +542,18 @@ def main():
     # quality (outside the timed region)
     res_q = rg.run(membership, compute_modularity=1, **opts)
 
+    # the autotuner on this graph (outside the timed region): its choice and time to result
+    tune = None
+    if not args.no_autotune:
+        t_tune = time.time()
+        best, tlog = rg.autotune(membership, **opts)
+        chosen = next(e for e in tlog if all(e[k] == v for k, v in best.items()))
+        tune = {"best": best, "best_ms_to_result": chosen["ms"], "best_iterations": chosen["iterations"],
+                "best_modularity": chosen["modularity"], "start_ms_to_result": tlog[0]["ms"],
+                "start_modularity": tlog[0]["modularity"], "candidates": len(tlog),
+                "tuning_s": time.time() - t_tune,
+                "objective": "time to result, modularity >= Q_start*(1-0.005)-0.001 (rak_graph_autotune)"}
+
     # end to end through the C ABI with host buffers in pinned memory
     # the host CSR arrays are page-locked in place (no second copy)
     cudart = torch.cuda.cudart()
@@ -592,7 +613,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
-                "gpu_launches": 3 * args.steps, "batched": batched, "serving": serving,
+                "gpu_launches": 3 * args.steps, "batched": batched, "serving": serving, "autotune": tune,
                 "run": {"iterations": last.iterations, "traversed_edges_per_step": last.traversed_edges,
                         "processed_vertices_per_step": last.processed_vertices,
                         "moved_vertices_per_step": last.moved_vertices, "loop_ms": last.loop_ms,

@@ -85,9 +85,9 @@ typedef struct rak_options {
   int32_t pickless_step;      /* -1: mode default; 0: never; k: iterations l%k==0 only move to
                                  smaller labels (inc/rakLowmemCuda.hxx:473-476) */
   int32_t check_on_pickless;  /* -1: mode default; 1: tolerance tested on pickless iterations */
-  int32_t lane_max;           /* 0: default; split layout, one lane per vertex up to this degree */
-  int32_t hub_min;            /* 0: default; vertices above this degree are split into chunks */
-  int32_t hub_chunk;          /* 0: default; edges per chunk of a split vertex */
+  int32_t lane_max;           /* 0: default [256]; split layout, one lane per vertex up to this degree */
+  int32_t hub_min;            /* 0: default [65536]; vertices above this degree are split into chunks */
+  int32_t hub_chunk;          /* 0: default [8192]; edges per chunk of a split vertex */
   int32_t validate;           /* 1: check the CSR on the device first [1] */
   int32_t compute_modularity; /* 1: fill rak_result.modularity (FP64 kernel) [0] */
   int32_t start_iteration;    /* iteration index of the first step (pickless schedule) [0] */
@@ -203,6 +203,41 @@ rak_status rak_batch_capture(rak_ctx *ctx, rak_batch *b, const uint32_t *q, cons
 rak_status rak_batch_replay(rak_ctx *ctx, rak_batch *b);
 /* FP64 modularity of every graph (membership: device, local labels); q: host, `graphs` entries. */
 rak_status rak_batch_modularity_f64(rak_ctx *ctx, rak_batch *b, const uint32_t *membership, double *q);
+
+/* ---- autotuning ------------------------------------------------------------------------------ */
+/* Picks lane_max / hub_min (degree thresholds), hub_chunk (the split-vertex tile) and slots (MG
+ * slot count) by running the graph or batch: coordinate descent from `base` over the values in the
+ * space, one dimension at a time, keeping the fastest run to convergence whose FP64 modularity
+ * (the mean over graphs for a batch) is at least Q_base * (1 - quality_rel) - quality_abs.
+ * No reference counterpart (the reference fixes these at compile time). */
+typedef struct rak_tune_space {
+  int32_t lane_max[8];  int32_t n_lane_max;   /* [32 64 128 256] */
+  int32_t hub_min[8];   int32_t n_hub_min;    /* [4096 8192 16384 32768 65536] */
+  int32_t hub_chunk[8]; int32_t n_hub_chunk;  /* [2048 4096 8192 16384] */
+  int32_t slots[5];     int32_t n_slots;      /* [4 8 16] */
+  int32_t repeats;                            /* timed runs per candidate, best kept [2] */
+  int32_t reserved;
+  double quality_rel, quality_abs;            /* [0.005, 0.001] */
+} rak_tune_space;
+
+typedef struct rak_tune_entry {  /* one candidate that was run */
+  int32_t lane_max, hub_min, hub_chunk, slots;
+  int32_t iterations, accepted;  /* accepted: passed the quality gate */
+  double ms;                     /* best time to result */
+  double modularity;
+  double edges_per_s;            /* traversed edges per second of that run */
+} rak_tune_entry;
+
+void rak_tune_space_default(rak_tune_space *sp);
+/* membership: device buffer of the graph's n labels, used by the runs. log (may be NULL) receives
+ * up to log_cap entries; *log_len (may be NULL) the number of candidates run. */
+rak_status rak_graph_autotune(rak_ctx *ctx, rak_graph *gr, const rak_options *base, const rak_tune_space *space,
+                              uint32_t *membership, rak_options *best, rak_tune_entry *log, int32_t log_cap,
+                              int32_t *log_len);
+/* The same for a batch of `graphs` graphs (membership: device, the batch's n labels). */
+rak_status rak_batch_autotune(rak_ctx *ctx, rak_batch *b, int64_t graphs, const rak_options *base,
+                              const rak_tune_space *space, uint32_t *membership, rak_options *best,
+                              rak_tune_entry *log, int32_t log_cap, int32_t *log_len);
 
 /* ---- serving: continuous batching of requests --------------------------------------------- */
 /* A request loop (its own host thread) that keeps admitted graphs resident on the device, admits

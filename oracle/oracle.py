@@ -75,7 +75,7 @@ _sig(_o, "orc_serial_run", C.c_int, C.POINTER(orc_csr), C.c_int, C.c_int, C.c_do
 _sig(_o, "orc_modularity", C.c_double, C.POINTER(orc_csr), P)
 
 # Layout defaults of the product (rak_internal.hpp DEFAULT_LANE_MAX / HUB_MIN / HUB_CHUNK).
-DEFAULT_LAYOUT = (128, 8192, 4096)
+DEFAULT_LAYOUT = (256, 65536, 8192)   # the library's defaults (lane_max, hub_min, hub_chunk)
 
 
 class Graph:

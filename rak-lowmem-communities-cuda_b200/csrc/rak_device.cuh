@@ -25,6 +25,7 @@ __device__ __forceinline__ void sk_clear(Sketch<S> &s) {
 // Weighted Misra-Gries accumulate with the reference CPU rule (inc/rakLowmem.hxx:63-89): add x to
 // every slot keyed c; otherwise the LAST zero-weight slot takes (c, x); otherwise every weight
 // drops by x, clamped at zero. Only adds, subtracts and max: bit-identical to the CPU.
+// Hits (the common case once labels settle) leave early; the miss path runs only when needed.
 template <int S>
 __device__ __forceinline__ void mg_acc(Sketch<S> &s, uint32_t c, float x) {
   bool hit = false;

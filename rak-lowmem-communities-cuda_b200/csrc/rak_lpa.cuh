@@ -16,6 +16,15 @@
 #include "rak_device.cuh"
 #include "rak_internal.hpp"
 
+// Edges loaded ahead per lane in the scan pipeline, and the resident blocks per SM the register
+// budget is sized for.
+#ifndef RAK_SCAN_BATCH
+#define RAK_SCAN_BATCH 4
+#endif
+#ifndef RAK_MIN_BLOCKS
+#define RAK_MIN_BLOCKS 3
+#endif
+
 namespace rak {
 
 struct Counters {
@@ -47,7 +56,7 @@ template <int S, bool UNIT>
 __device__ __forceinline__ void scan_range(Sketch<S> &sk, uint32_t u, int64_t e, int64_t ee, int st,
                                            const uint32_t *tgt, const float *wt, const uint32_t *vin,
                                            uint32_t base) {
-  constexpr int B = 4;
+  constexpr int B = RAK_SCAN_BATCH;
   uint32_t t[B];
   float w[B];
 #pragma unroll
@@ -96,21 +105,42 @@ __device__ __forceinline__ void rescan_range(Sketch<S> &sk, uint32_t u, int64_t 
   }
 }
 
+
 // Marks neighbours e, e+st, ... < ee of a moved vertex u as affected (inc/rakCuda.hxx:95-103),
 // except u itself (the reference CPU loop clears u after marking, inc/rakLowmem.hxx:203,209).
+// Pipelined in batches of eight: the next batch's targets load while this batch is stored.
+// TEST: store a flag only if it reads as clear (from L2, ld.cg, not a possibly stale L1 line). A
+// random byte store costs the L2 a partial write, about half the rate of a read, and most
+// neighbours of a moved vertex are flagged already; but the read adds a dependent round trip to
+// the marking of each vertex. Measured on R-MAT (scale 22-24, ef 32): testing pays in the
+// split-vertex marking pass and for the Boyer-Moore sketch, not inside Misra-Gries items.
+template <bool TEST>
 __device__ __forceinline__ void mark_range(uint32_t u, int64_t e, int64_t ee, int st, const uint32_t *tgt,
                                            uint8_t *fout, uint32_t base) {
-  for (; e + 3 * int64_t(st) < ee; e += 4 * int64_t(st)) {
-    const uint32_t v0 = base + __ldg(tgt + e), v1 = base + __ldg(tgt + e + st),
-                   v2 = base + __ldg(tgt + e + 2 * st), v3 = base + __ldg(tgt + e + 3 * st);
-    if (v0 != u) fout[v0] = 1;
-    if (v1 != u) fout[v1] = 1;
-    if (v2 != u) fout[v2] = 1;
-    if (v3 != u) fout[v3] = 1;
+  constexpr int MB = 8;
+  uint32_t v[MB];
+#pragma unroll
+  for (int j = 0; j < MB; ++j) {
+    const int64_t x = e + int64_t(j) * st;
+    v[j] = x < ee ? base + __ldg(tgt + x) : u;
   }
-  for (; e < ee; e += st) {
-    const uint32_t v = base + __ldg(tgt + e);
-    if (v != u) fout[v] = 1;
+  while (e < ee) {
+    uint32_t f[MB];
+#pragma unroll
+    for (int j = 0; j < MB; ++j) f[j] = v[j] == u ? 1u : (TEST ? uint32_t(__ldcg(fout + v[j])) : 0u);
+    const int64_t en = e + int64_t(MB) * st;
+    uint32_t v2[MB];
+#pragma unroll
+    for (int j = 0; j < MB; ++j) {
+      const int64_t x = en + int64_t(j) * st;
+      v2[j] = x < ee ? base + __ldg(tgt + x) : u;
+    }
+#pragma unroll
+    for (int j = 0; j < MB; ++j)
+      if (!f[j]) fout[v[j]] = 1;
+#pragma unroll
+    for (int j = 0; j < MB; ++j) v[j] = v2[j];
+    e = en;
   }
 }
 
@@ -236,7 +266,7 @@ __device__ __forceinline__ void lane_batch(const LpaArgs &a, const G_<O> &g, con
     cnt.changed += 1;
     cnt.moved_edges += (unsigned long long)(ee - eb);
     count_move<BATCH>(a, gi, it);
-    mark_range(u, eb, ee, 1, g.tgt, fout, base);
+    mark_range<S == 1>(u, eb, ee, 1, g.tgt, fout, base);
   }
 }
 
@@ -281,7 +311,7 @@ __device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, 
     }
     if (moved) { cnt.changed += 1; cnt.moved_edges += (unsigned long long)(ee - eb); count_move<BATCH>(a, gi, it); }
   }
-  if (moved) mark_range(u, eb + s, ee, G, g.tgt, fout, base);
+  if (moved) mark_range<S == 1>(u, eb + s, ee, G, g.tgt, fout, base);
 }
 
 // Region 0: one chunk of a split vertex per item. In the synchronous exact mode chunk 0's warp
@@ -316,7 +346,7 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
       if (active) { cnt.processed += 1; cnt.edges += (unsigned long long)(ee - eb); }
       if (moved) { cnt.changed += 1; cnt.moved_edges += (unsigned long long)(ee - eb); count_move<BATCH>(a, gi, it); }
     }
-    if (moved) mark_range(u, eb + lane, ee, 32, g.tgt, fout, base);
+    if (moved) mark_range<S == 1>(u, eb + lane, ee, 32, g.tgt, fout, base);
     return;
   } else {
     bool active;
@@ -408,7 +438,7 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
 }
 
 template <int S, int MODE, class O, bool UNIT, bool BATCH>
-__global__ void __launch_bounds__(256, 3) lpa_run(const LpaArgs a) {
+__global__ void __launch_bounds__(256, RAK_MIN_BLOCKS) lpa_run(const LpaArgs a) {
   const G_<O> g{static_cast<const O *>(a.off), a.tgt, a.wt};
   RunState *rs = static_cast<RunState *>(a.rs);
   const int lane = threadIdx.x & 31;
@@ -492,7 +522,7 @@ __global__ void __launch_bounds__(256, 3) lpa_run(const LpaArgs a) {
         const int64_t cb = eb + j * a.hub_chunk, ce = cb + a.hub_chunk < ee ? cb + a.hub_chunk : ee;
         uint32_t gi, base;
         graph_of<BATCH>(a, u, gi, base);
-        mark_range(u, cb + lane, ce, 32, g.tgt, fout, base);
+        mark_range<true>(u, cb + lane, ce, 32, g.tgt, fout, base);
       }
     }
     if constexpr (BATCH) {

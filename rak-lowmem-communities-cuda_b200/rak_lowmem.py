@@ -74,6 +74,19 @@ class rak_server_stats(C.Structure):
                 ("pack_ms", C.c_double), ("plan_host_ms", C.c_double), ("enqueue_ms", C.c_double)]
 
 
+class rak_tune_space(C.Structure):
+    _fields_ = [("lane_max", C.c_int32 * 8), ("n_lane_max", C.c_int32), ("hub_min", C.c_int32 * 8),
+                ("n_hub_min", C.c_int32), ("hub_chunk", C.c_int32 * 8), ("n_hub_chunk", C.c_int32),
+                ("slots", C.c_int32 * 5), ("n_slots", C.c_int32), ("repeats", C.c_int32), ("reserved", C.c_int32),
+                ("quality_rel", C.c_double), ("quality_abs", C.c_double)]
+
+
+class rak_tune_entry(C.Structure):
+    _fields_ = [("lane_max", C.c_int32), ("hub_min", C.c_int32), ("hub_chunk", C.c_int32), ("slots", C.c_int32),
+                ("iterations", C.c_int32), ("accepted", C.c_int32), ("ms", C.c_double), ("modularity", C.c_double),
+                ("edges_per_s", C.c_double)]
+
+
 class rak_host_csr(C.Structure):
     _fields_ = [("n", C.c_int64), ("m", C.c_int64), ("offsets", C.c_void_p), ("targets", C.c_void_p),
                 ("weights", C.c_void_p), ("truth", C.c_void_p)]
@@ -109,6 +122,11 @@ _sig("rak_batch_capture", C.c_int, P, P, P, C.POINTER(rak_options), P)
 _sig("rak_batch_replay", C.c_int, P, P)
 _sig("rak_batch_modularity_f64", C.c_int, P, P, P, P)
 _sig("rak_server_options_default", None, C.POINTER(rak_server_options))
+_sig("rak_tune_space_default", None, C.POINTER(rak_tune_space))
+_sig("rak_graph_autotune", C.c_int, P, P, C.POINTER(rak_options), C.POINTER(rak_tune_space), P,
+     C.POINTER(rak_options), C.POINTER(rak_tune_entry), C.c_int32, C.POINTER(C.c_int32))
+_sig("rak_batch_autotune", C.c_int, P, P, C.c_int64, C.POINTER(rak_options), C.POINTER(rak_tune_space), P,
+     C.POINTER(rak_options), C.POINTER(rak_tune_entry), C.c_int32, C.POINTER(C.c_int32))
 _sig("rak_server_create", C.c_int, P, C.POINTER(rak_server_options), C.POINTER(P))
 _sig("rak_server_submit", C.c_int, P, C.POINTER(rak_csr), C.POINTER(C.c_uint64))
 _sig("rak_server_wait", C.c_int, P, C.c_uint64, C.c_double, P, C.POINTER(rak_result))
@@ -148,6 +166,34 @@ def options(**kw) -> rak_options:
             raise TypeError(f"unknown option {k}")
         setattr(o, k, v)
     return o
+
+
+def tune_space(**kw) -> rak_tune_space:
+    """rak_tune_space_default, overridden by keyword: lane_max / hub_min / hub_chunk / slots take a
+    list of values, the other fields a number."""
+    sp = rak_tune_space()
+    _lib.rak_tune_space_default(C.byref(sp))
+    for k, v in kw.items():
+        if k in ("lane_max", "hub_min", "hub_chunk", "slots"):
+            arr = getattr(sp, k)
+            if len(v) > len(arr):
+                raise ValueError(f"at most {len(arr)} values for {k}")
+            for i, x in enumerate(v):
+                arr[i] = int(x)
+            setattr(sp, "n_" + k, len(v))
+        elif hasattr(sp, k):
+            setattr(sp, k, v)
+        else:
+            raise TypeError(f"unknown tuning field {k}")
+    return sp
+
+
+_OPTION_KEYS = ("lane_max", "hub_min", "hub_chunk", "slots")
+
+
+def _tune_out(best, log, n):
+    return ({k: getattr(best, k) for k in _OPTION_KEYS},
+            [{f[0]: getattr(log[i], f[0]) for f in rak_tune_entry._fields_} for i in range(min(n, len(log)))])
 
 
 @dataclass
@@ -390,6 +436,16 @@ class ResidentGraph:
     def device_bytes(self) -> int:
         return _lib.rak_graph_device_bytes(self._g)
 
+    def autotune(self, membership, space=None, **base_opts):
+        """rak_graph_autotune: returns ({lane_max, hub_min, hub_chunk, slots} of the best run, the
+        list of candidates run)."""
+        o, best = options(**base_opts), rak_options()
+        log, n = (rak_tune_entry * 64)(), C.c_int32(0)
+        sp = space if space is not None else tune_space()
+        _check(_lib.rak_graph_autotune(self.ctx.handle, self._g, C.byref(o), C.byref(sp), membership.data_ptr(),
+                                       C.byref(best), log, 64, C.byref(n)), self.ctx.handle)
+        return _tune_out(best, log, n.value)
+
     def run(self, membership, q=None, **opts) -> Result:
         o = options(**opts)
         r = rak_result()
@@ -469,6 +525,15 @@ class Batch:
 
     def __del__(self):
         self.close()
+
+    def autotune(self, membership, space=None, **base_opts):
+        """rak_batch_autotune (quality: mean modularity over the graphs); see ResidentGraph.autotune."""
+        o, best = options(**base_opts), rak_options()
+        log, n = (rak_tune_entry * 64)(), C.c_int32(0)
+        sp = space if space is not None else tune_space()
+        _check(_lib.rak_batch_autotune(self.ctx.handle, self._b, self.graphs, C.byref(o), C.byref(sp),
+                                       membership.data_ptr(), C.byref(best), log, 64, C.byref(n)), self.ctx.handle)
+        return _tune_out(best, log, n.value)
 
     def launch(self, membership, q=None, **opts):
         o = options(**opts)

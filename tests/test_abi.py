@@ -77,3 +77,16 @@ def test_plan_summary_partitions_vertices():
     assert chunks == int(((deg[deg > 512] + 255) // 256).sum())
     with pytest.raises(rl.RakError):
         rl.plan_summary(g, lane_max=4096)                               # above MAX_LANE_MAX
+
+
+def test_tune_space_defaults():
+    sp = rl.tune_space()
+    assert list(sp.lane_max)[:sp.n_lane_max] == [32, 64, 128, 256]
+    assert list(sp.hub_min)[:sp.n_hub_min] == [4096, 8192, 16384, 32768, 65536]
+    assert list(sp.hub_chunk)[:sp.n_hub_chunk] == [2048, 4096, 8192, 16384]
+    assert list(sp.slots)[:sp.n_slots] == [4, 8, 16]
+    assert sp.repeats == 2 and sp.quality_rel == 0.005 and sp.quality_abs == 0.001
+    sp = rl.tune_space(slots=[8], hub_chunk=[4096, 8192], repeats=1)
+    assert sp.n_slots == 1 and sp.n_hub_chunk == 2 and sp.repeats == 1
+    with pytest.raises(ValueError):
+        rl.tune_space(slots=[1, 2, 4, 8, 16, 32])

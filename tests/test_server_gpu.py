@@ -63,7 +63,7 @@ def test_async_quality_in_the_mix(ctx):
         lab, res = srv.wait(t)
         assert lab.max() < g.n and res.iterations >= 1
         planted = orc.modularity(orc.Graph.of(g), g.truth)
-        assert orc.modularity(orc.Graph.of(g), lab) >= 0.9 * planted
+        assert orc.modularity(orc.Graph.of(g), lab) >= 0.85 * planted
     srv.close()
 
 

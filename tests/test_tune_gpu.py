@@ -1,0 +1,55 @@
+"""Autotuner (rak_graph_autotune / rak_batch_autotune): the search starts from the caller's options,
+every candidate stays inside the space, the choice passes the quality gate and is the fastest
+accepted candidate, and running with it gives a valid labelling."""
+import numpy as np
+import pytest
+
+import rak_lowmem as rl
+
+pytestmark = pytest.mark.gpu
+
+
+def check_log(best, log, sp):
+    assert log[0]["accepted"] == 1
+    q_floor = log[0]["modularity"] * (1 - sp.quality_rel) - sp.quality_abs
+    accepted = [e for e in log if e["accepted"]]
+    assert all(e["modularity"] >= q_floor for e in accepted)
+    assert all(e["modularity"] < q_floor for e in log if not e["accepted"])
+    fastest = min(accepted, key=lambda e: e["ms"])
+    assert {k: fastest[k] for k in best} == best
+    for e in log[1:]:
+        assert e["lane_max"] in list(sp.lane_max)[:sp.n_lane_max] + [128]
+        assert e["slots"] in list(sp.slots)[:sp.n_slots] + [8]
+
+
+def test_graph_autotune():
+    import torch
+    g = rl.gen_sbm(60000, 60, 16.0, 1000.0, seed=5)   # about 94% of edges inside blocks
+    sp = rl.tune_space(repeats=1, hub_min=[4096, 16384], hub_chunk=[2048, 4096])
+    with rl.Context(0) as ctx:
+        rg = rl.ResidentGraph(ctx, g)
+        mem = torch.empty(g.n, dtype=torch.int32, device="cuda")
+        best, log = rg.autotune(mem, space=sp, slots=8)
+        check_log(best, log, sp)
+        assert len(log) >= 1 + 3 + 1 + 1 + 2
+        res = rg.run(mem, compute_modularity=1, **best)
+        lab = mem.cpu().numpy()
+        assert lab.min() >= 0 and lab.max() < g.n and res.modularity > 0.5
+        rg.close()
+
+
+def test_batch_autotune():
+    import torch
+    gs = [rl.gen_sbm(2000 + 500 * i, 10, 12.0, 1000.0, seed=i) for i in range(6)] + [rl.gen_rmat(11, 8, seed=9)]
+    hb = rl.HostBatch.concat(gs, weighted=False)
+    sp = rl.tune_space(repeats=1, lane_max=[64, 128], hub_min=[8192], hub_chunk=[4096])
+    with rl.Context(0) as ctx:
+        b = rl.Batch(ctx, hb)
+        mem = torch.empty(hb.n, dtype=torch.int32, device="cuda")
+        best, log = b.autotune(mem, space=sp)
+        check_log(best, log, sp)
+        b.launch(mem, **best)
+        b.results()
+        q = b.modularity(mem)
+        assert np.all(np.asarray(q)[:6] > 0.5)
+        b.close()
