@@ -56,13 +56,20 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-def make_graph(spec, threads=0):
+def make_graph(spec, threads=0, ctx=None):
+    """The workload's graph on the host, and (R-MAT with a context) the same graph built on the
+    device by rak_gen_rmat_device -- bit-identical to the host generator, and seconds instead of
+    minutes at scale 27. Returns (host graph, device graph or None)."""
     import rak_lowmem as rl
     if spec["kind"] == "rmat":
+        if ctx is not None:
+            dg = rl.gen_rmat_device(ctx, spec["scale"], spec["ef"], 0.57, 0.19, 0.19, 42, spec["w"][0], spec["w"][1],
+                                    offset_bits=spec["off_bits"])
+            return dg.to_host(), dg
         g = rl.gen_rmat(spec["scale"], spec["ef"], 0.57, 0.19, 0.19, 42, spec["w"][0], spec["w"][1], threads)
     else:
         g = rl.gen_lattice(spec["width"], spec["height"], spec["p_delete"], spec["shortcut"], 42, threads)
-    return g
+    return g, None
 
 
 def describe(name, spec, g):
@@ -171,7 +178,7 @@ def run_reference(args, spec, world, rank):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as orc
     threads = os.cpu_count() or 1
-    g = make_graph(spec, threads)
+    g, _ = make_graph(spec, threads)
     og = orc.Graph.of(g)
     log(f"[reference] graph n={g.n} m={g.m}; rakLowmemStaticOmp<MG8,rescan> first iteration, {threads} threads")
     times = []
@@ -480,17 +487,19 @@ def main():
         torch.cuda.synchronize()
 
     threads = max(1, (os.cpu_count() or 1) // world)
-    t0 = time.time()
-    g = make_graph(spec, threads)
-    if spec["off_bits"] == 32:
-        g = g.with_offsets32()
-    log(f"[rank {rank}] graph n={g.n} m={g.m} generated in {time.time() - t0:.1f}s")
     ctx = rl.Context(local)
     # A dedicated stream: the library's work and the timing events share it.
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
-    rg = rl.ResidentGraph(ctx, g)
+    t0 = time.time()
+    g, dg = make_graph(spec, threads, ctx)
+    if spec["off_bits"] == 32:
+        g = g.with_offsets32()
+    log(f"[rank {rank}] graph n={g.n} m={g.m} generated in {time.time() - t0:.1f}s "
+        f"({'on the device' if dg is not None else 'on the host'})")
+    # the resident graph: the device-built arrays when there are some, else a copy of the host graph
+    rg = rl.ResidentGraph(ctx, dg.csr if dg is not None else g)
     membership = torch.empty(g.n, dtype=torch.int32, device="cuda")
     opts = dict(slots=args.slots)
 
@@ -564,6 +573,8 @@ def main():
     out_host = torch.empty(g.n, dtype=torch.int32).pin_memory()
     e2e_edges, e2e_time = 0, 0.0
     rg.close()
+    if dg is not None:
+        dg.close()
     for i in range(args.e2e_steps + 1):
         barrier()
         s0 = torch.cuda.Event(enable_timing=True)

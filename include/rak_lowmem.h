@@ -329,6 +329,18 @@ typedef struct rak_host_csr {
  * NULL weights. threads <= 0: all cores. */
 rak_status rak_gen_rmat(int scale, double edge_factor, double a, double b, double c, uint64_t seed,
                         float w_lo, float w_hi, int threads, rak_host_csr *out);
+/* The same symmetric R-MAT built on ctx's device, bit-identical to rak_gen_rmat for the same
+ * arguments (same samples, sorted duplicate-free adjacency, same weights; unit weights leave
+ * weights NULL). offset_bits 32 or 64. Arrays are allocated on the device; free them with
+ * rak_device_csr_free. Needs about 16 bytes of device memory per sampled edge direction while it
+ * builds (a scale-27, edge-factor-16 graph: ~70 GB). No reference counterpart (the reference reads
+ * its graphs from files). */
+rak_status rak_gen_rmat_device(rak_ctx *ctx, int scale, double edge_factor, double a, double b, double c,
+                               uint64_t seed, float w_lo, float w_hi, int32_t offset_bits, rak_csr *out);
+rak_status rak_device_csr_free(rak_csr *g);
+/* Copies a device-located CSR into newly allocated host arrays (offsets widened to 64 bits); free
+ * them with rak_host_csr_free. */
+rak_status rak_device_csr_to_host(const rak_csr *g, rak_host_csr *out);
 /* Planted-partition SBM: n vertices in k equal blocks, expected degree avg_degree, ratio
  * p_in/p_out; unit weights; truth[] holds the planted block of each vertex. */
 rak_status rak_gen_sbm(int64_t n, int64_t k, double avg_degree, double in_out_ratio, uint64_t seed,

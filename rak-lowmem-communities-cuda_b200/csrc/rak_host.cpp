@@ -129,7 +129,8 @@ struct rak_graph {
   int64_t *hub_first = nullptr;
   int64_t nhub = 0, nchunks = 0;
   rak::Regions rg{};
-  uint64_t graph_bytes = 0, plan_bytes = 0;
+  uint64_t graph_bytes = 0, plan_bytes = 0;  // allocated by the library: graph copy, plan
+  uint64_t ref_bytes = 0;                    // the caller's device arrays a device-located graph uses
   float plan_ms = 0, h2d_ms = 0;
   size_t off_cap = 0, tgt_cap = 0, wt_cap = 0;  // bytes allocated for an owned copy
   void *wt_alloc = nullptr;                      // owned weight buffer (wt may be null: unit weights)
@@ -394,6 +395,8 @@ rak_status graph_create(rak_ctx *ctx, const rak_csr *g, const Resolved &r, Track
     gr->off = g->offsets;
     gr->tgt = g->targets;
     gr->wt = g->weights;
+    gr->ref_bytes = ob + uint64_t(g->m) * 4 * (g->weights ? 2 : 1);
+    if (tr) tr->add(gr->ref_bytes);
   } else {
     if (r.validate) {
       rak_status s = rak_csr_validate_host(g);
@@ -649,7 +652,7 @@ rak_status rak_graph_run(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const r
   RAK_CHECK(resolve(ctx, o, &r));
   RAK_TRY(ctx, cudaSetDevice(ctx->device));
   Tracker tr;
-  tr.add(gr->graph_bytes + gr->plan_bytes);
+  tr.add(gr->graph_bytes + gr->ref_bytes + gr->plan_bytes);
   rak_result tmp{};
   rak_result *rr = res ? res : &tmp;
   std::memset(rr, 0, sizeof(*rr));
@@ -796,6 +799,82 @@ rak_status rak_modularity_f64(rak_ctx *ctx, const rak_csr *g, const uint32_t *me
   if (g->weights && m > 0) RAK_TRY(ctx, cudaMemcpyAsync(wt.p, g->weights, size_t(m) * 4, cudaMemcpyHostToDevice, ctx->stream));
   if (n > 0) RAK_TRY(ctx, cudaMemcpyAsync(lab.p, membership, size_t(n) * 4, cudaMemcpyHostToDevice, ctx->stream));
   return modularity_dev(ctx, off.p, g->offset_bits == 64, tgt.as<uint32_t>(), wt.as<float>(), n, lab.as<uint32_t>(), nullptr, q);
+}
+
+rak_status rak_gen_rmat_device(rak_ctx *ctx, int scale, double edge_factor, double a, double b, double c,
+                               uint64_t seed, float w_lo, float w_hi, int32_t offset_bits, rak_csr *out) {
+  cudaGetLastError();  // drop a stale error left by an unrelated failed call
+  if (!ctx || !out || scale < 1 || scale > 31 || !(edge_factor > 0) || a < 0 || b < 0 || c < 0 || a + b + c > 1.0 ||
+      w_hi < w_lo || (offset_bits != 32 && offset_bits != 64))
+    return RAK_ERR_INVALID_ARGUMENT;
+  std::memset(out, 0, sizeof(*out));
+  RAK_TRY(ctx, cudaSetDevice(ctx->device));
+  const int64_t samples = int64_t(std::llround(double(int64_t(1) << scale) * edge_factor));
+  const uint32_t tA = uint32_t(std::lround(a * 65536.0));
+  const uint32_t tAB = uint32_t(std::lround((a + b) * 65536.0));
+  const uint32_t tABC = uint32_t(std::lround((a + b + c) * 65536.0));
+  const bool weighted = !(w_lo == 1.0f && w_hi == 1.0f);
+  rak::GenDeviceOut g{};
+  const cudaError_t e = rak::gen_rmat_device(scale, samples, seed, tA, tAB, tABC, weighted, w_lo, w_hi,
+                                             offset_bits == 64, ctx->stream, &g);
+  if (e == cudaErrorInvalidValue) {
+    set_err(ctx, "more edges than 32-bit offsets can index");
+    return RAK_ERR_INVALID_ARGUMENT;
+  }
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    set_err(ctx, "device memory: the build needs about 16 bytes per sampled edge direction");
+    return RAK_ERR_OUT_OF_MEMORY;
+  }
+  RAK_TRY(ctx, e);
+  out->n = g.n;
+  out->m = g.m;
+  out->offset_bits = offset_bits;
+  out->location = RAK_DEVICE;
+  out->offsets = g.offsets;
+  out->targets = g.targets;
+  out->weights = g.weights;
+  return RAK_OK;
+}
+
+rak_status rak_device_csr_to_host(const rak_csr *g, rak_host_csr *out) {
+  cudaGetLastError();  // drop a stale error left by an unrelated failed call
+  if (!g || !out || g->location != RAK_DEVICE || check_csr_shape(nullptr, g) != RAK_OK) return RAK_ERR_INVALID_ARGUMENT;
+  std::memset(out, 0, sizeof(*out));
+  const int64_t n = g->n, m = g->m;
+  out->offsets = static_cast<int64_t *>(std::malloc(size_t(n + 1) * 8));
+  out->targets = static_cast<uint32_t *>(std::malloc(size_t(std::max<int64_t>(m, 1)) * 4));
+  if (g->weights) out->weights = static_cast<float *>(std::malloc(size_t(std::max<int64_t>(m, 1)) * 4));
+  if (!out->offsets || !out->targets || (g->weights && !out->weights)) {
+    rak_host_csr_free(out);
+    return RAK_ERR_OUT_OF_MEMORY;
+  }
+  cudaError_t e = cudaSuccess;
+  if (g->offset_bits == 64) {
+    e = cudaMemcpy(out->offsets, g->offsets, size_t(n + 1) * 8, cudaMemcpyDeviceToHost);
+  } else {
+    std::vector<int32_t> o32(size_t(n + 1));
+    e = cudaMemcpy(o32.data(), g->offsets, size_t(n + 1) * 4, cudaMemcpyDeviceToHost);
+    for (int64_t u = 0; u <= n; ++u) out->offsets[u] = o32[size_t(u)];
+  }
+  if (e == cudaSuccess && m > 0) e = cudaMemcpy(out->targets, g->targets, size_t(m) * 4, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && m > 0 && g->weights) e = cudaMemcpy(out->weights, g->weights, size_t(m) * 4, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    rak_host_csr_free(out);
+    return RAK_ERR_CUDA;
+  }
+  out->n = n;
+  out->m = m;
+  return RAK_OK;
+}
+
+rak_status rak_device_csr_free(rak_csr *g) {
+  if (!g || g->location != RAK_DEVICE) return RAK_ERR_INVALID_ARGUMENT;
+  cudaFree(const_cast<void *>(g->offsets));
+  cudaFree(const_cast<uint32_t *>(g->targets));
+  cudaFree(const_cast<float *>(g->weights));
+  std::memset(g, 0, sizeof(*g));
+  return RAK_OK;
 }
 
 rak_status rak_csr_validate_host(const rak_csr *g) {

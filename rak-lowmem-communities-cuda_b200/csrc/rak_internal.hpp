@@ -128,6 +128,16 @@ cudaError_t launch_modularity(const void *off, bool off64, const uint32_t *tgt, 
 
 // Batches of graphs (rak_kernels.cu).
 cudaError_t launch_fill_f32(float *p, int64_t count, float v, cudaStream_t st);
+// Symmetric R-MAT on the device (rak_gen_device.cu); arrays allocated with cudaMalloc.
+struct GenDeviceOut {
+  void *offsets;
+  uint32_t *targets;
+  float *weights;
+  int64_t n, m;
+  uint64_t peak_bytes;  // device bytes held at the peak of the build
+};
+cudaError_t gen_rmat_device(int scale, int64_t samples, uint64_t seed, uint32_t tA, uint32_t tAB, uint32_t tABC,
+                            bool weighted, float w_lo, float w_hi, bool off64, cudaStream_t st, GenDeviceOut *out);
 // One graph to pack into a batch CSR from device memory (k_gather_graphs).
 struct GatherItem {
   const void *off;       // n + 1 offsets, int64 if off64 else int32

@@ -142,6 +142,10 @@ _sig("rak_gen_sbm", C.c_int, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_u
 _sig("rak_gen_lattice", C.c_int, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_uint64, C.c_int,
      C.POINTER(rak_host_csr))
 _sig("rak_host_csr_free", None, C.POINTER(rak_host_csr))
+_sig("rak_gen_rmat_device", C.c_int, P, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64,
+     C.c_float, C.c_float, C.c_int32, C.POINTER(rak_csr))
+_sig("rak_device_csr_free", C.c_int, C.POINTER(rak_csr))
+_sig("rak_device_csr_to_host", C.c_int, C.POINTER(rak_csr), C.POINTER(rak_host_csr))
 _sig("rak_csr_validate_host", C.c_int, C.POINTER(rak_csr))
 _sig("rak_plan_summary_host", C.c_int, C.POINTER(rak_csr), C.POINTER(rak_options), C.POINTER(C.c_int64),
      C.POINTER(C.c_int64))
@@ -291,6 +295,37 @@ def gen_rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=42, w_lo=1.0, w
     h = rak_host_csr()
     _check(_lib.rak_gen_rmat(scale, edge_factor, a, b, c, seed, w_lo, w_hi, threads, C.byref(h)))
     return _wrap_host(h)
+
+
+class DeviceGraph:
+    """A CSR generated on the device by the library (rak_gen_rmat_device); `csr` is its rak_csr
+    (location DEVICE). Freed by close()."""
+
+    def __init__(self, csr: rak_csr):
+        self.csr = csr
+        self.n, self.m = int(csr.n), int(csr.m)
+        self.weighted = bool(csr.weights)
+
+    def to_host(self) -> HostGraph:
+        h = rak_host_csr()
+        _check(_lib.rak_device_csr_to_host(C.byref(self.csr), C.byref(h)))
+        return _wrap_host(h)
+
+    def close(self):
+        if _lib is not None and self.csr.offsets:
+            _lib.rak_device_csr_free(C.byref(self.csr))
+
+    def __del__(self):
+        self.close()
+
+
+def gen_rmat_device(ctx, scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=42, w_lo=1.0, w_hi=1.0,
+                    offset_bits=64) -> DeviceGraph:
+    """rak_gen_rmat_device: the graph gen_rmat builds, built on ctx's device."""
+    c_ = rak_csr()
+    _check(_lib.rak_gen_rmat_device(ctx.handle, scale, edge_factor, a, b, c, seed, w_lo, w_hi, offset_bits,
+                                    C.byref(c_)), ctx.handle)
+    return DeviceGraph(c_)
 
 
 def gen_sbm(n, k, avg_degree=16.0, in_out_ratio=20.0, seed=42, threads=0) -> HostGraph:
