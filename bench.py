@@ -165,6 +165,19 @@ def algorithmic_bytes(res, off_bytes, weighted):
             + 4 * res.moved_vertices + 5 * res.moved_edges)
 
 
+def whole_job(dist, seconds, units, device):
+    """Aggregate over ranks: the slowest rank's time (max) and every rank's units (sum); the
+    whole-job rate is units / time. Without a process group, the local values."""
+    if dist is None:
+        return float(seconds), float(units)
+    import torch
+    t = torch.tensor([float(seconds)], dtype=torch.float64, device=device)
+    u = torch.tensor([float(units)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(u.item())
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -521,15 +534,7 @@ def main():
         barrier()
     elapsed = ev0.elapsed_time(ev1) / 1e3
     edges = sum(r.traversed_edges for r in results)
-    t_max = elapsed
-    total_edges = edges
-    if pg:
-        t = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        t_max = float(t.item())
-        e = torch.tensor([edges], dtype=torch.float64, device="cuda")
-        pg.all_reduce(e, op=pg.ReduceOp.SUM)
-        total_edges = float(e.item())
+    t_max, total_edges = whole_job(pg, elapsed, edges, "cuda")
     value = total_edges / t_max
 
     # roofline of the persistent LPA kernel, from the runs just timed
@@ -594,12 +599,8 @@ def main():
             e2e_edges += r.traversed_edges
     for arr in host_arrays:
         cudart.cudaHostUnregister(arr.ctypes.data)
-    e2e_t = torch.tensor([e2e_time], dtype=torch.float64, device="cuda")
-    e2e_e = torch.tensor([float(e2e_edges)], dtype=torch.float64, device="cuda")
-    if pg:
-        pg.all_reduce(e2e_t, op=pg.ReduceOp.MAX)
-        pg.all_reduce(e2e_e, op=pg.ReduceOp.SUM)
-    e2e = {"value": float(e2e_e.item()) / float(e2e_t.item()), "unit": UNIT,
+    e2e_t, e2e_e = whole_job(pg, e2e_time, e2e_edges, "cuda")
+    e2e = {"value": e2e_e / e2e_t, "unit": UNIT,
            "h2d_bytes_per_step": graph_bytes(g, spec["off_bits"]), "d2h_bytes_per_step": g.n * 4,
            "path": "rak_lowmem_cuda (C ABI) with pinned host CSR: upload, plan, run, membership read-back",
            "steps": args.e2e_steps}

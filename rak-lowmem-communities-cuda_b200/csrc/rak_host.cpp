@@ -475,8 +475,10 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
   a.sk_keys = b.skk.as<uint32_t>(); a.sk_wts = b.skw.as<float>();
   a.stats = b.stats.as<unsigned long long>(); a.rs = b.rs.p;
   a.iters = r.iters; a.start_iter = r.start; a.tolerance = r.tol; a.pickless_step = r.pickless;
-  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.timeout_ns = 20LL * 1000 * 1000 * 1000;
+  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n); a.timeout_ns = 20LL * 1000 * 1000 * 1000;
 
+  // the kernel's module is loaded here, not inside the timed region
+  if (r.iters > 0) RAK_TRY(ctx, rak::prepare_lpa(r.slots, r.mode, gr->off64, gr->wt == nullptr, false));
   Events ev;
   float t_init = 0, t_mark = 0, t_all = 0, t_loop = 0;
   rak::RunStateHost hs{};
@@ -757,7 +759,7 @@ rak_status rak_graph_step(rak_ctx *ctx, rak_graph *gr, const rak_options *o, int
   a.sk_keys = b.skk.as<uint32_t>(); a.sk_wts = b.skw.as<float>();
   a.stats = b.stats.as<unsigned long long>(); a.rs = b.rs.p;
   a.iters = 1; a.start_iter = iteration; a.tolerance = r.tol; a.pickless_step = r.pickless;
-  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.timeout_ns = 20LL * 1000 * 1000 * 1000;
+  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n); a.timeout_ns = 20LL * 1000 * 1000 * 1000;
   int grid = 0;
   RAK_TRY(ctx, rak::launch_lpa(a, r.slots, r.mode, gr->off64, st, &grid));
   unsigned long long s[rak::STATS_STRIDE] = {};
@@ -917,6 +919,7 @@ namespace {
 rak_status batch_prepare(rak_ctx *ctx, rak_batch *b, const Resolved &r) {
   rak_graph *gr = b->g;
   if (!same_layout(gr->ly, r.ly)) RAK_CHECK(build_plan(ctx, gr, r.ly, nullptr));
+  if (r.iters > 0) RAK_TRY(ctx, rak::prepare_lpa(r.slots, r.mode, true, gr->wt == nullptr, true));
   const int64_t n = gr->n, G = b->ngraphs;
   const bool sync = r.mode != RAK_MODE_ASYNC;
   const int iters = std::max(r.iters, 1);
@@ -977,7 +980,7 @@ rak_status batch_enqueue(rak_ctx *ctx, rak_batch *b, const uint32_t *q, const Re
     a.giters = b->giters.as<int32_t>(); a.gchanged = b->gchanged.as<unsigned long long>();
     a.running = b->running.as<unsigned int>(); a.ngraphs = G; a.grid_cap = grid_cap;
     a.iters = r.iters; a.start_iter = r.start; a.tolerance = r.tol; a.pickless_step = r.pickless;
-    a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.timeout_ns = 20LL * 1000 * 1000 * 1000;
+    a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n); a.timeout_ns = 20LL * 1000 * 1000 * 1000;
     int grid = 0;
     RAK_TRY(ctx, rak::launch_lpa(a, r.slots, r.mode, true, st, &grid, true));
   }

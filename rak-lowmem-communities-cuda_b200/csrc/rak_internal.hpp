@@ -88,6 +88,7 @@ struct LpaArgs {
   unsigned int *running;        // per iteration: graphs still running after it
   int64_t ngraphs;
   int grid_cap;                 // at most this many blocks (0: as many as fit), to share the GPU
+  int mark_test;                // neighbour marking reads a flag before storing it (mark_test_for)
   int iters;
   int start_iter;
   double tolerance;
@@ -110,6 +111,13 @@ cudaError_t launch_lpa(const LpaArgs &a, int slots, int mode, bool off64, cudaSt
 // Per-slot-count instantiations (rak_lpa_s*.cu).
 template <int S>
 cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, bool batch, cudaStream_t st, int *grid_out);
+template <int S>
+cudaError_t resolve_lpa_slots(int mode, bool off64, bool unit, bool batch, const void **fn, int *per_sm);
+// Whether neighbour marking inside work items reads each flag before storing it: measured to pay
+// for the Boyer-Moore sketch on graphs of 2^20 vertices and more, and to cost otherwise.
+inline int mark_test_for(int slots, int64_t n) { return slots == 1 && n >= (int64_t(1) << 20) ? 1 : 0; }
+// Loads and resolves the kernel a run will launch (outside its timed region).
+cudaError_t prepare_lpa(int slots, int mode, bool off64, bool unit, bool batch);
 
 // Plan and utility kernels (rak_kernels.cu).
 cudaError_t launch_validate(const void *off, bool off64, const uint32_t *tgt, int64_t n, int64_t m,

@@ -13,6 +13,10 @@
 // the next item from a per-iteration counter, so the load balances dynamically. Sketches live in
 // registers, one per lane.
 #pragma once
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "rak_device.cuh"
 #include "rak_internal.hpp"
 
@@ -109,11 +113,14 @@ __device__ __forceinline__ void rescan_range(Sketch<S> &sk, uint32_t u, int64_t 
 // Marks neighbours e, e+st, ... < ee of a moved vertex u as affected (inc/rakCuda.hxx:95-103),
 // except u itself (the reference CPU loop clears u after marking, inc/rakLowmem.hxx:203,209).
 // Pipelined in batches of eight: the next batch's targets load while this batch is stored.
-// TEST: store a flag only if it reads as clear (from L2, ld.cg, not a possibly stale L1 line). A
+// test: store a flag only if it reads as clear (from L2, ld.cg, not a possibly stale L1 line). A
 // random byte store costs the L2 a partial write, about half the rate of a read, and most
 // neighbours of a moved vertex are flagged already; but the read adds a dependent round trip to
-// the marking of each vertex. Measured on R-MAT (scale 22-24, ef 32): testing pays in the
-// split-vertex marking pass and for the Boyer-Moore sketch, not inside Misra-Gries items.
+// the marking of each vertex. Measured: testing pays in the split-vertex marking pass and for the
+// Boyer-Moore sketch on graphs of a million vertices and more (R-MAT scale 22-24: +15%), not
+// inside Misra-Gries items (-16%) nor on small graphs, whose flags stay in L1 (SBM 100k: 2.6x
+// slower). The Boyer-Moore kernels choose per launch (LpaArgs::mark_test); the Misra-Gries ones
+// never test inside items.
 template <bool TEST>
 __device__ __forceinline__ void mark_range(uint32_t u, int64_t e, int64_t ee, int st, const uint32_t *tgt,
                                            uint8_t *fout, uint32_t base) {
@@ -141,6 +148,18 @@ __device__ __forceinline__ void mark_range(uint32_t u, int64_t e, int64_t ee, in
 #pragma unroll
     for (int j = 0; j < MB; ++j) v[j] = v2[j];
     e = en;
+  }
+}
+
+// Neighbour marking inside work items (see mark_range).
+template <int S>
+__device__ __forceinline__ void mark_item(const LpaArgs &a, uint32_t u, int64_t e, int64_t ee, int st,
+                                          const uint32_t *tgt, uint8_t *fout, uint32_t base) {
+  if constexpr (S == 1) {
+    if (a.mark_test) mark_range<true>(u, e, ee, st, tgt, fout, base);
+    else mark_range<false>(u, e, ee, st, tgt, fout, base);
+  } else {
+    mark_range<false>(u, e, ee, st, tgt, fout, base);
   }
 }
 
@@ -266,7 +285,7 @@ __device__ __forceinline__ void lane_batch(const LpaArgs &a, const G_<O> &g, con
     cnt.changed += 1;
     cnt.moved_edges += (unsigned long long)(ee - eb);
     count_move<BATCH>(a, gi, it);
-    mark_range<S == 1>(u, eb, ee, 1, g.tgt, fout, base);
+    mark_item<S>(a, u, eb, ee, 1, g.tgt, fout, base);
   }
 }
 
@@ -311,7 +330,7 @@ __device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, 
     }
     if (moved) { cnt.changed += 1; cnt.moved_edges += (unsigned long long)(ee - eb); count_move<BATCH>(a, gi, it); }
   }
-  if (moved) mark_range<S == 1>(u, eb + s, ee, G, g.tgt, fout, base);
+  if (moved) mark_item<S>(a, u, eb + s, ee, G, g.tgt, fout, base);
 }
 
 // Region 0: one chunk of a split vertex per item. In the synchronous exact mode chunk 0's warp
@@ -346,7 +365,7 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
       if (active) { cnt.processed += 1; cnt.edges += (unsigned long long)(ee - eb); }
       if (moved) { cnt.changed += 1; cnt.moved_edges += (unsigned long long)(ee - eb); count_move<BATCH>(a, gi, it); }
     }
-    if (moved) mark_range<S == 1>(u, eb + lane, ee, 32, g.tgt, fout, base);
+    if (moved) mark_item<S>(a, u, eb + lane, ee, 32, g.tgt, fout, base);
     return;
   } else {
     bool active;
@@ -574,10 +593,12 @@ __global__ void __launch_bounds__(256, RAK_MIN_BLOCKS) lpa_run(const LpaArgs a) 
   }
 }
 
+// The kernel instantiation for a launch and its resident blocks per SM, cached per (function,
+// device). The first query of an instantiation loads its module (CUDA loads modules lazily, which
+// can take a millisecond), so runs resolve before their timed region (prepare_lpa).
 template <int S>
-cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, bool batch, cudaStream_t st, int *grid_out) {
+cudaError_t resolve_lpa_slots(int mode, bool off64, bool unit, bool batch, const void **fn_out, int *per_sm_out) {
   const void *fn = nullptr;
-  const bool unit = a.wt == nullptr;
 #define RAK_PICK(M, O, U, B)                                                          \
   if (mode == M && off64 == (sizeof(O) == 8) && unit == U && batch == B)             \
     fn = reinterpret_cast<const void *>(&lpa_run<S, M, O, U, B>);
@@ -589,12 +610,38 @@ cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, bool batch,
 #undef RAK_PICK_MODE
 #undef RAK_PICK
   if (!fn) return cudaErrorInvalidValue;
-  int dev = 0, sms = 0, per_sm = 0;
+  int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, int> cache;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    const auto it = cache.find({fn, dev});
+    if (it != cache.end()) {
+      *fn_out = fn;
+      *per_sm_out = it->second;
+      return cudaSuccess;
+    }
+  }
+  int per_sm = 0;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0)) != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  std::lock_guard<std::mutex> lk(mu);
+  cache[{fn, dev}] = per_sm;
+  *fn_out = fn;
+  *per_sm_out = per_sm;
+  return cudaSuccess;
+}
+
+template <int S>
+cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, bool batch, cudaStream_t st, int *grid_out) {
+  const void *fn = nullptr;
+  int per_sm = 0, dev = 0, sms = 0;
+  cudaError_t e = resolve_lpa_slots<S>(mode, off64, a.wt == nullptr, batch, &fn, &per_sm);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
   const int64_t warps_needed = a.rg.ibegin[NREG] > 0 ? a.rg.ibegin[NREG] : 1;
   int64_t grid = int64_t(per_sm) * sms;
   const int64_t want = (warps_needed + 7) / 8;

@@ -1,0 +1,62 @@
+"""The replica path of bench.py (--gpus N under torch.distributed.run), exercised on CPU with the
+gloo backend and 2 ranks: the whole-job aggregation takes the slowest rank's time and the sum of
+every rank's work, and the reference arm runs on rank 0 only (the other ranks exit without work)."""
+import os
+import socket
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out):
+    import datetime
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        assert bench.dist_setup() == (world, rank, rank)
+        seconds = 1.0 + rank            # rank 1 is the slowest
+        units = 100 * (rank + 1)
+        t, u = bench.whole_job(dist, seconds, units, "cpu")
+        out.put((rank, t, u))
+        # the reference arm: rank 0 alone does work; others return at once
+        class A:
+            steps, warmup, workload = 1, 3, "rmat16_ef16"
+        if rank != 0:
+            assert bench.run_reference(A, bench.WORKLOADS["rmat16_ef16"], world, rank) is None
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_whole_job_aggregation_two_ranks():
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    got = sorted(out.get(timeout=5) for _ in range(2))
+    for rank, t, u in got:
+        assert t == pytest.approx(2.0) and u == pytest.approx(300.0)
+
+
+def test_single_process_is_local():
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.whole_job(None, 2.5, 7, "cpu") == (2.5, 7.0)
