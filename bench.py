@@ -576,10 +576,14 @@ def main():
         assert int(cudart.cudaHostRegister(arr.ctypes.data, arr.nbytes, 0)) == 0, "cudaHostRegister failed"
     hg = g
     out_host = torch.empty(g.n, dtype=torch.int32).pin_memory()
-    e2e_edges, e2e_time = 0, 0.0
+    e2e_edges, e2e_time, e2e_parts = 0, 0.0, []
     rg.close()
     if dg is not None:
         dg.close()
+    # repeated calls: the context keeps the call's device buffers mapped between calls
+    # (rak_ctx_set_memory_keep); every call still uploads the whole graph and reads labels back
+    keep_bytes = int(1.5 * graph_bytes(g, spec["off_bits"])) + (64 << 20)
+    ctx.set_memory_keep(keep_bytes)
     for i in range(args.e2e_steps + 1):
         barrier()
         s0 = torch.cuda.Event(enable_timing=True)
@@ -597,12 +601,17 @@ def main():
         if i > 0:   # the first call warms the allocator
             e2e_time += s0.elapsed_time(s1) / 1e3
             e2e_edges += r.traversed_edges
+            e2e_parts.append({"call_ms": s0.elapsed_time(s1), "h2d_ms": r.h2d_ms, "plan_ms": r.plan_ms,
+                              "run_ms": r.time_ms, "d2h_ms": r.d2h_ms})
     for arr in host_arrays:
         cudart.cudaHostUnregister(arr.ctypes.data)
+    ctx.set_memory_keep(0)
     e2e_t, e2e_e = whole_job(pg, e2e_time, e2e_edges, "cuda")
     e2e = {"value": e2e_e / e2e_t, "unit": UNIT,
            "h2d_bytes_per_step": graph_bytes(g, spec["off_bits"]), "d2h_bytes_per_step": g.n * 4,
-           "path": "rak_lowmem_cuda (C ABI) with pinned host CSR: upload, plan, run, membership read-back",
+           "path": "rak_lowmem_cuda (C ABI) with pinned host CSR: upload, plan, run, membership read-back; "
+                   "rak_ctx_set_memory_keep(%d) so repeated calls reuse mapped device memory" % keep_bytes,
+           "calls": [{k: round(v, 2) for k, v in p.items()} for p in e2e_parts],
            "steps": args.e2e_steps}
 
     cpu = None

@@ -131,6 +131,12 @@ rak_status rak_ctx_create(int device, rak_ctx **out);
 rak_status rak_ctx_destroy(rak_ctx *ctx);
 /* Work is issued on `stream` (a cudaStream_t; NULL = the context's own stream). */
 rak_status rak_ctx_set_stream(rak_ctx *ctx, void *stream);
+/* Device memory the context keeps mapped between rak_lowmem_cuda calls (default 0: every call
+ * releases what it allocated, as the reference does). With bytes > 0 the call's graph copy and
+ * working buffers come from a stream-ordered pool of the context that keeps up to `bytes` after
+ * the call, so repeated calls on graphs of similar size skip mapping and unmapping them.
+ * No reference counterpart. */
+rak_status rak_ctx_set_memory_keep(rak_ctx *ctx, uint64_t bytes);
 /* Text of the last error on this context (empty if none). */
 const char *rak_ctx_last_error(const rak_ctx *ctx);
 

@@ -33,6 +33,8 @@ struct rak_ctx {
   cudaStream_t own = nullptr;
   int sms = 0;
   std::string err;
+  cudaMemPool_t pool = nullptr;  // one-shot runs allocate here while keep > 0 (rak_ctx_set_memory_keep)
+  uint64_t keep = 0;
 };
 
 namespace rak_host_detail {
@@ -398,16 +400,16 @@ rak_status graph_create(rak_ctx *ctx, const rak_csr *g, const Resolved &r, Track
     gr->ref_bytes = ob + uint64_t(g->m) * 4 * (g->weights ? 2 : 1);
     if (tr) tr->add(gr->ref_bytes);
   } else {
-    if (r.validate) {
-      rak_status s = rak_csr_validate_host(g);
-      if (s != RAK_OK) { set_err(ctx, "invalid CSR (host check)"); return fail(s); }
-    }
+    // a host graph is checked on the device once uploaded (below): the copies touch only the
+    // n + 1 offsets and m edges it declares, and the device reads it ~100x faster than the host
     gr->owns = true;
     Events ev;
     void *po = nullptr, *pt = nullptr, *pw = nullptr;
-    cudaError_t e = cudaMalloc(&po, ob);
-    if (e == cudaSuccess) e = cudaMalloc(&pt, size_t(std::max<int64_t>(g->m, 1)) * 4);
-    if (e == cudaSuccess && g->weights) e = cudaMalloc(&pw, size_t(std::max<int64_t>(g->m, 1)) * 4);
+    gr->arrays_pooled = rak_host_detail::thread_pool().pool != nullptr;
+    cudaError_t e = rak_host_detail::dev_alloc(&po, ob, &gr->arrays_fs);
+    if (e == cudaSuccess) e = rak_host_detail::dev_alloc(&pt, size_t(std::max<int64_t>(g->m, 1)) * 4, &gr->arrays_fs);
+    if (e == cudaSuccess && g->weights)
+      e = rak_host_detail::dev_alloc(&pw, size_t(std::max<int64_t>(g->m, 1)) * 4, &gr->arrays_fs);
     gr->off = po; gr->tgt = static_cast<uint32_t *>(pt); gr->wt = static_cast<float *>(pw);
     gr->off_cap = ob;
     gr->tgt_cap = size_t(std::max<int64_t>(g->m, 1)) * 4;
@@ -425,7 +427,7 @@ rak_status graph_create(rak_ctx *ctx, const rak_csr *g, const Resolved &r, Track
     if (e != cudaSuccess) return fail(from_cuda(ctx, e, "copy graph to device"));
     gr->h2d_ms = ev.ms(0, 1);
   }
-  if (g->location == RAK_DEVICE && r.validate) {
+  if (r.validate) {
     DevBuf bad;
     cudaError_t e = bad.alloc(4, tr);
     unsigned int hbad = 0;
@@ -611,6 +613,10 @@ rak_status rak_ctx_create(int device, rak_ctx **out) {
 rak_status rak_ctx_destroy(rak_ctx *ctx) {
   if (!ctx) return RAK_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
+  if (ctx->pool) {
+    cudaDeviceSynchronize();
+    cudaMemPoolDestroy(ctx->pool);
+  }
   if (ctx->own) cudaStreamDestroy(ctx->own);
   delete ctx;
   return RAK_OK;
@@ -619,6 +625,28 @@ rak_status rak_ctx_destroy(rak_ctx *ctx) {
 rak_status rak_ctx_set_stream(rak_ctx *ctx, void *stream) {
   if (!ctx) return RAK_ERR_INVALID_ARGUMENT;
   ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own;
+  return RAK_OK;
+}
+
+rak_status rak_ctx_set_memory_keep(rak_ctx *ctx, uint64_t bytes) {
+  cudaGetLastError();  // drop a stale error left by an unrelated failed call
+  if (!ctx) return RAK_ERR_INVALID_ARGUMENT;
+  RAK_TRY(ctx, cudaSetDevice(ctx->device));
+  if (!ctx->pool) {
+    if (bytes == 0) return RAK_OK;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = ctx->device;
+    RAK_TRY(ctx, cudaMemPoolCreate(&ctx->pool, &props));
+  }
+  uint64_t keep = bytes;
+  RAK_TRY(ctx, cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  if (bytes == 0) {  // back to cudaMalloc/cudaFree: a pool that keeps nothing re-maps on every call
+    RAK_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    RAK_TRY(ctx, cudaMemPoolTrimTo(ctx->pool, 0));
+  }
+  ctx->keep = bytes;
   return RAK_OK;
 }
 
@@ -677,6 +705,9 @@ rak_status rak_lowmem_cuda(rak_ctx *ctx, const rak_csr *g, const uint32_t *q, co
   rak_result *rr = res ? res : &tmp;
   std::memset(rr, 0, sizeof(*rr));
   rr->modularity = std::numeric_limits<double>::quiet_NaN();
+  // with a context pool, this call's buffers are stream-ordered allocations from it (kept mapped
+  // between calls up to the pool's threshold); otherwise cudaMalloc/cudaFree
+  rak_host_detail::PoolScope scope(ctx->keep > 0 ? ctx->pool : nullptr, ctx->stream);
   Tracker tr;
   rak_graph *gr = nullptr;
   RAK_CHECK(graph_create(ctx, g, r, &tr, &gr));

@@ -106,6 +106,7 @@ _sig("rak_options_default", None, C.POINTER(rak_options))
 _sig("rak_ctx_create", C.c_int, C.c_int, C.POINTER(P))
 _sig("rak_ctx_destroy", C.c_int, P)
 _sig("rak_ctx_set_stream", C.c_int, P, P)
+_sig("rak_ctx_set_memory_keep", C.c_int, P, C.c_uint64)
 _sig("rak_ctx_last_error", C.c_char_p, P)
 _sig("rak_lowmem_cuda", C.c_int, P, C.POINTER(rak_csr), P, C.POINTER(rak_options), P, C.POINTER(rak_result))
 _sig("rak_graph_create", C.c_int, P, C.POINTER(rak_csr), C.POINTER(rak_options), C.POINTER(P))
@@ -393,6 +394,10 @@ class Context:
 
     def set_stream(self, stream_ptr: Optional[int]):
         _check(_lib.rak_ctx_set_stream(self._c, stream_ptr), self._c)
+
+    def set_memory_keep(self, nbytes: int):
+        """rak_ctx_set_memory_keep: device bytes kept mapped between lowmem() calls."""
+        _check(_lib.rak_ctx_set_memory_keep(self._c, int(nbytes)), self._c)
 
     def last_error(self) -> str:
         return _lib.rak_ctx_last_error(self._c).decode()

@@ -17,9 +17,10 @@ def check_log(best, log, sp):
     assert all(e["modularity"] < q_floor for e in log if not e["accepted"])
     fastest = min(accepted, key=lambda e: e["ms"])
     assert {k: fastest[k] for k in best} == best
+    start = log[0]
     for e in log[1:]:
-        assert e["lane_max"] in list(sp.lane_max)[:sp.n_lane_max] + [128]
-        assert e["slots"] in list(sp.slots)[:sp.n_slots] + [8]
+        assert e["lane_max"] in list(sp.lane_max)[:sp.n_lane_max] + [start["lane_max"]]
+        assert e["slots"] in list(sp.slots)[:sp.n_slots] + [start["slots"]]
 
 
 def test_graph_autotune():
