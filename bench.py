@@ -396,9 +396,9 @@ def serving_leg(ctx, rates, seconds, threads, seed=11):
                 arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
                 picks = np.where(rng.random(count) < 0.02, len(pool), rng.integers(0, len(pool), count))
                 srv = rl.Server(ctx, slots=2, validate=0)
-                # warm-up, untimed: grows the server's pools and loads its kernels (a few pool graphs
-                # and the large one, alone and together)
-                for ks in ([0, 1, 2, 3], [len(pool)], [4, len(pool), 5]):
+                # warm-up, untimed: grows both launch slots' pools and loads the kernels (the large
+                # graph twice at once, so each slot runs one; then pool graphs with and without it)
+                for ks in ([len(pool), len(pool)], [0, 1, 2, 3], [4, len(pool), 5]):
                     for t in [(srv.submit_device(arena[k][1], arena[k][0]) if arm == "arena"
                                else srv.submit(graphs[k])) for k in ks]:
                         srv.wait(t, timeout=600.0)
