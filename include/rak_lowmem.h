@@ -355,6 +355,13 @@ rak_status rak_gen_sbm(int64_t n, int64_t k, double avg_degree, double in_out_ra
  * p_delete, plus shortcut_frac * (edges) random undirected shortcuts; unit weights. */
 rak_status rak_gen_lattice(int64_t width, int64_t height, double p_delete, double shortcut_frac,
                            uint64_t seed, int threads, rak_host_csr *out);
+/* Reads a Matrix Market coordinate file as the reference's driver does (inc/mtx.hxx
+ * readMtxOmpW, inc/symmetrize.hxx symmetrizeOmpU, main.cxx:116-119): 1-based entries become 0-based
+ * vertices (n = max(rows, cols)); "symmetric"/"skew-symmetric" files store both directions; with
+ * weighted, the third column is the weight and 0 reads as 1 (else weights are NULL: unit); a
+ * repeated (u, v) keeps its last occurrence in the file; with symmetrize, a missing reverse edge
+ * is added with the same weight. threads <= 0: all cores. */
+rak_status rak_read_mtx(const char *path, int weighted, int symmetrize, int threads, rak_host_csr *out);
 void rak_host_csr_free(rak_host_csr *g);
 
 /* Host-side CSR check (same rules as the device check): RAK_OK or RAK_ERR_INVALID_CSR. */

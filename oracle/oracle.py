@@ -192,7 +192,22 @@ def ref_cpu():
         _sig(_ref, "ref_modularity", C.c_double, C.c_int64, P, P, P, P)
         _sig(_ref, "ref_sync_step", C.c_int64, C.c_int64, P, P, P, C.c_int, C.c_int, C.c_int, P, P, P, P)
         _sig(_ref, "ref_sketch_stream", C.c_int, C.c_int, C.c_int64, P, P, P, P)
+        _sig(_ref, "ref_read_mtx", C.c_int, C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_int64),
+             C.POINTER(C.c_int64), P, P, P)
     return _ref
+
+
+def ref_read_mtx(path, weighted=False, symmetrize=True):
+    """The reference driver's loading of an MTX file (readMtxOmpW + symmetrizeOmpU), 0-based:
+    (offsets int64, targets uint32, weights float32 or None)."""
+    n, m = C.c_int64(0), C.c_int64(0)
+    ref_cpu().ref_read_mtx(str(path).encode(), int(weighted), int(symmetrize), C.byref(n), C.byref(m), None, None, None)
+    off = np.empty(n.value + 1, np.int64)
+    tgt = np.empty(max(m.value, 1), np.uint32)
+    wt = np.empty(max(m.value, 1), np.float32)
+    ref_cpu().ref_read_mtx(str(path).encode(), int(weighted), int(symmetrize), C.byref(n), C.byref(m),
+                           off.ctypes.data, tgt.ctypes.data, wt.ctypes.data)
+    return off, tgt[:m.value], (wt[:m.value] if weighted else None)
 
 
 def ref_sketch_stream(slots, comm, wts):

@@ -17,6 +17,9 @@
 #include <vector>
 #include <omp.h>
 #include "_main.hxx"
+#include "Graph.hxx"
+#include "mtx.hxx"
+#include "symmetrize.hxx"
 #include "properties.hxx"
 #include "rak.hxx"
 #include "rakLowmem.hxx"
@@ -196,6 +199,32 @@ int ref_sketch_stream(int slots, int64_t len, const uint32_t *comm, const float 
   ST(2) ST(4) ST(8) ST(16) ST(32)
 #undef ST
   return -1;
+}
+
+// The reference driver's graph loading (main.cxx:116-119): readMtxOmpW into DiGraph<uint32_t, None,
+// float>, then symmetrizeOmpU unless the caller says the file is symmetric. The result comes back
+// 0-based (vertex k+1 of the reference is k here), targets sorted per vertex. Two passes: with
+// off == nullptr only *n and *m are set.
+int ref_read_mtx(const char *path, int weighted, int symmetrize, int64_t *n, int64_t *m, int64_t *off,
+                 uint32_t *tgt, float *wt) {
+  DiGraph<uint32_t, None, float> x;
+  readMtxOmpW(x, path, weighted != 0);
+  if (symmetrize) symmetrizeOmpU(x);
+  const int64_t span = int64_t(x.span());
+  *n = span > 0 ? span - 1 : 0;
+  *m = int64_t(x.size());
+  if (!off) return 0;
+  int64_t e = 0;
+  off[0] = 0;
+  for (int64_t u = 1; u < span; ++u) {
+    x.forEachEdge(uint32_t(u), [&](auto v, auto w) {
+      tgt[e] = uint32_t(v) - 1;
+      if (wt) wt[e] = float(w);
+      ++e;
+    });
+    off[u] = e;
+  }
+  return 0;
 }
 
 }  // extern "C"

@@ -146,6 +146,7 @@ _sig("rak_host_csr_free", None, C.POINTER(rak_host_csr))
 _sig("rak_gen_rmat_device", C.c_int, P, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64,
      C.c_float, C.c_float, C.c_int32, C.POINTER(rak_csr))
 _sig("rak_device_csr_free", C.c_int, C.POINTER(rak_csr))
+_sig("rak_read_mtx", C.c_int, C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(rak_host_csr))
 _sig("rak_device_csr_to_host", C.c_int, C.POINTER(rak_csr), C.POINTER(rak_host_csr))
 _sig("rak_csr_validate_host", C.c_int, C.POINTER(rak_csr))
 _sig("rak_plan_summary_host", C.c_int, C.POINTER(rak_csr), C.POINTER(rak_options), C.POINTER(C.c_int64),
@@ -295,6 +296,13 @@ def _check(st: int, ctx=None):
 def gen_rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=42, w_lo=1.0, w_hi=1.0, threads=0) -> HostGraph:
     h = rak_host_csr()
     _check(_lib.rak_gen_rmat(scale, edge_factor, a, b, c, seed, w_lo, w_hi, threads, C.byref(h)))
+    return _wrap_host(h)
+
+
+def read_mtx(path, weighted=False, symmetrize=True, threads=0) -> HostGraph:
+    """rak_read_mtx: a Matrix Market coordinate file as the reference's driver reads it."""
+    h = rak_host_csr()
+    _check(_lib.rak_read_mtx(str(path).encode(), int(weighted), int(symmetrize), threads, C.byref(h)))
     return _wrap_host(h)
 
 
