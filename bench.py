@@ -230,6 +230,24 @@ def cpu_baseline(g, budget_s=20.0):
                       f"on the same graph, best of {len(times)}"}
 
 
+def cpu_baseline_gve(g, budget_s=20.0):
+    """The reference's GVE-LPA (rakStaticOmp, per-thread hashtables) on the host cores: first
+    iteration over the graph, best of up to three within the budget."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    if not orc.have_ref_cpu():
+        return None
+    threads = os.cpu_count() or 1
+    og = orc.Graph.of(g)
+    times = []
+    t0 = time.time()
+    while not times or (time.time() - t0 < budget_s and len(times) < 3):
+        _, _, tms = orc.ref_gve_omp(og, tolerance=0.05, max_iterations=1, threads=threads)
+        times.append(tms / 1e3)
+    return {"value": g.m / min(times), "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"first iteration of rakStaticOmp (GVE-LPA) on the same graph, best of {len(times)}"}
+
+
 def nmi(a, b):
     """Normalised mutual information (arithmetic mean normalisation) of two labellings."""
     a = np.unique(np.asarray(a), return_inverse=True)[1]
@@ -614,9 +632,10 @@ def main():
            "calls": [{k: round(v, 2) for k, v in p.items()} for p in e2e_parts],
            "steps": args.e2e_steps}
 
-    cpu = None
+    cpu = cpu_gve = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(g)
+        cpu_gve = cpu_baseline_gve(g)
     batched = None
     if args.batch_graphs > 0:
         batched = batched_leg(ctx, args.batch_graphs, 3, threads, stream)
@@ -633,7 +652,8 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+                "roofline": roofline, "cpu_baseline": cpu, "cpu_baseline_gve_lpa": cpu_gve, "e2e": e2e,
+                "clocks": clk.summary(),
                 "gpu_launches": 3 * args.steps, "batched": batched, "serving": serving, "autotune": tune,
                 "run": {"iterations": last.iterations, "traversed_edges_per_step": last.traversed_edges,
                         "processed_vertices_per_step": last.processed_vertices,

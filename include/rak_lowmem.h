@@ -92,7 +92,13 @@ typedef struct rak_options {
   int32_t compute_modularity; /* 1: fill rak_result.modularity (FP64 kernel) [0] */
   int32_t start_iteration;    /* iteration index of the first step (pickless schedule) [0] */
   const uint8_t *initial_flags; /* NULL: every vertex affected; else n flags in the csr's location */
-  int64_t reserved[8];
+  int32_t sketch_rule;        /* -1 or 0: mode default; 1: the reference CPU sketch rules (last free
+                                 slot, clamped decrement, linear argmax, move if w > 0); 2: its GPU
+                                 rules (first free slot, unclamped, tournament argmax, move if
+                                 w != 0, Boyer-Moore from the own label). ASYNC uses 2, SYNC 1,
+                                 SYNC_SPLIT either [1] */
+  int32_t reserved32;
+  int64_t reserved[7];
 } rak_options;
 
 typedef struct rak_result {

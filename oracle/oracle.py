@@ -46,7 +46,7 @@ class orc_layout(C.Structure):
 class orc_opts(C.Structure):
     _fields_ = [("slots", C.c_int), ("rescan", C.c_int), ("split", C.c_int), ("layout", orc_layout),
                 ("tolerance", C.c_double), ("max_iterations", C.c_int), ("pickless_step", C.c_int),
-                ("check_on_pickless", C.c_int)]
+                ("check_on_pickless", C.c_int), ("gpu_rule", C.c_int)]
 
 
 class orc_sketch(C.Structure):
@@ -66,6 +66,8 @@ _sig(_o, "orc_mg_accumulate", None, C.POINTER(orc_sketch), C.c_int, C.c_uint32, 
 _sig(_o, "orc_bm_accumulate", None, C.POINTER(orc_sketch), C.c_uint32, C.c_float)
 _sig(_o, "orc_sketch_merge", None, C.POINTER(orc_sketch), C.POINTER(orc_sketch), C.c_int)
 _sig(_o, "orc_sketch_choose", None, C.POINTER(orc_sketch), C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_float))
+_sig(_o, "orc_mg_accumulate_gpu", None, C.POINTER(orc_sketch), C.c_int, C.c_uint32, C.c_float)
+_sig(_o, "orc_sketch_choose_gpu", None, C.POINTER(orc_sketch), C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_float))
 _sig(_o, "orc_choose", None, C.POINTER(orc_csr), C.POINTER(orc_opts), C.c_uint32, P, C.POINTER(C.c_uint32),
      C.POINTER(C.c_float))
 _sig(_o, "orc_sync_step", C.c_uint64, C.POINTER(orc_csr), C.POINTER(orc_opts), C.c_int, P, P, P, P,
@@ -95,9 +97,9 @@ class Graph:
 
 
 def make_opts(slots=8, rescan=0, split=0, layout=DEFAULT_LAYOUT, tolerance=0.05, max_iterations=20,
-              pickless_step=0, check_on_pickless=1) -> orc_opts:
+              pickless_step=0, check_on_pickless=1, gpu_rule=0) -> orc_opts:
     return orc_opts(slots, rescan, split, orc_layout(*layout), tolerance, max_iterations, pickless_step,
-                    check_on_pickless)
+                    check_on_pickless, gpu_rule)
 
 
 def sync_step(g, o: orc_opts, iteration, vcom_prev, aff_prev):
@@ -146,14 +148,17 @@ def choose(g, o: orc_opts, u, vcom):
 class Sketch:
     """A Misra-Gries (slots >= 2) or Boyer-Moore (slots == 1) sketch, for stream-level tests."""
 
-    def __init__(self, slots):
+    def __init__(self, slots, gpu_rule=False):
         self.slots = slots
+        self.gpu = gpu_rule
         self.s = orc_sketch()
         _o.orc_sketch_clear(C.byref(self.s), slots)
 
     def add(self, c, w):
         if self.slots == 1:
             _o.orc_bm_accumulate(C.byref(self.s), c, w)
+        elif self.gpu:
+            _o.orc_mg_accumulate_gpu(C.byref(self.s), self.slots, c, w)
         else:
             _o.orc_mg_accumulate(C.byref(self.s), self.slots, c, w)
         return self
@@ -164,7 +169,8 @@ class Sketch:
 
     def choose(self):
         c, w = C.c_uint32(0), C.c_float(0)
-        _o.orc_sketch_choose(C.byref(self.s), self.slots, C.byref(c), C.byref(w))
+        f = _o.orc_sketch_choose_gpu if self.gpu else _o.orc_sketch_choose
+        f(C.byref(self.s), self.slots, C.byref(c), C.byref(w))
         return int(c.value), float(w.value)
 
     def slots_list(self):
@@ -271,7 +277,8 @@ def have_ref_cuda() -> bool:
 
 
 def ref_lowmem_cuda(g, slots=8, repeat=1, tolerance=0.05, max_iterations=20, timeout=600):
-    """The reference's own GPU path rakLowmemStaticCuda<slots> run as a separate process."""
+    """The reference's own GPU path rakLowmemStaticCuda<slots> run as a separate process (slots 0:
+    the reference's ν-LPA, rakStaticCuda, with per-vertex hashtables)."""
     g = Graph.of(g)
     with tempfile.TemporaryDirectory() as d:
         gp, lp = os.path.join(d, "g.rakcsr"), os.path.join(d, "labels.bin")

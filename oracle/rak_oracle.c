@@ -9,6 +9,8 @@
  *   - sketch merge by re-accumulation  : inc/sketchCuda.hxx:150-158 (sketchMergeWarpCudU)
  *   - pickless rule                    : inc/rakLowmemCuda.hxx:473-487
  *   - modularity                       : inc/properties.hxx:123-126, 177-192
+ *   - GPU rule set (gpu_rule)          : inc/sketchCuda.hxx:73-108 (accumulate), 190-201 (argmax),
+ *                                        inc/rakLowmemCuda.hxx:41-43, 152, 306 (BM start, moves)
  * Floating point follows the reference exactly: float sketch weights, adds and subtracts only
  * (no multiply, so no contraction), double modularity.
  */
@@ -39,6 +41,31 @@ void orc_mg_accumulate(orc_sketch *s, int slots, uint32_t c, float w) {
   }
 }
 
+/* inc/sketchCuda.hxx:73-108 (sketchAccumulateWarpCudU, one sketch per thread): add w to every slot
+ * holding c; if none held it, the FIRST slot whose weight is exactly zero takes (c, w); if no slot
+ * is free, every weight drops by w, without a clamp. */
+void orc_mg_accumulate_gpu(orc_sketch *s, int slots, uint32_t c, float w) {
+  int has = 0;
+  for (int i = 0; i < slots; ++i)
+    if (s->k[i] == c) { s->w[i] += w; has = 1; }
+  if (has) return;
+  for (int i = 0; i < slots; ++i)
+    if (s->w[i] == 0.0f) { s->k[i] = c; s->w[i] = w; return; }
+  for (int i = 0; i < slots; ++i) s->w[i] -= w;
+}
+
+/* inc/sketchCuda.hxx:190-201: tournament -- at each level slot i takes slot i+ds when strictly
+ * heavier; the winner is slot 0, whatever its weight. */
+void orc_sketch_choose_gpu(const orc_sketch *s, int slots, uint32_t *c, float *w) {
+  uint32_t k[ORC_MAX_SLOTS];
+  float x[ORC_MAX_SLOTS];
+  for (int i = 0; i < slots; ++i) { k[i] = s->k[i]; x[i] = s->w[i]; }
+  for (int ds = slots / 2; ds >= 1; ds /= 2)
+    for (int i = 0; i < ds; ++i)
+      if (x[i + ds] > x[i]) { k[i] = k[i + ds]; x[i] = x[i + ds]; }
+  *c = k[0]; *w = x[0];
+}
+
 /* inc/rakLowmem.hxx:120-126: weighted Boyer-Moore vote held in slot 0. */
 void orc_bm_accumulate(orc_sketch *s, uint32_t c, float w) {
   if (c == s->k[0]) s->w[0] += w;
@@ -46,15 +73,19 @@ void orc_bm_accumulate(orc_sketch *s, uint32_t c, float w) {
   else { s->k[0] = c; s->w[0] = w; }
 }
 
-/* inc/sketchCuda.hxx:150-158: merge b into a by re-accumulating b's non-zero slots in order. */
-void orc_sketch_merge(orc_sketch *a, const orc_sketch *b, int slots) {
-  if (slots == 1) {
-    if (b->w[0] != 0.0f) orc_bm_accumulate(a, b->k[0], b->w[0]);
-    return;
-  }
-  for (int j = 0; j < slots; ++j)
-    if (b->w[j] != 0.0f) orc_mg_accumulate(a, slots, b->k[j], b->w[j]);
+static void acc_rule(orc_sketch *s, int slots, uint32_t c, float w, int gpu) {
+  if (slots == 1) orc_bm_accumulate(s, c, w);
+  else if (gpu) orc_mg_accumulate_gpu(s, slots, c, w);
+  else orc_mg_accumulate(s, slots, c, w);
 }
+
+static void merge_rule(orc_sketch *a, const orc_sketch *b, int slots, int gpu) {
+  for (int j = 0; j < slots; ++j)
+    if (b->w[j] != 0.0f) acc_rule(a, slots, b->k[j], b->w[j], gpu);
+}
+
+/* inc/sketchCuda.hxx:150-158: merge b into a by re-accumulating b's non-zero slots in order. */
+void orc_sketch_merge(orc_sketch *a, const orc_sketch *b, int slots) { merge_rule(a, b, slots, 0); }
 
 /* inc/rakLowmem.hxx:164-171: linear argmax, strict '>', starting from weight 0. */
 void orc_sketch_choose(const orc_sketch *s, int slots, uint32_t *c, float *w) {
@@ -65,25 +96,27 @@ void orc_sketch_choose(const orc_sketch *s, int slots, uint32_t *c, float *w) {
   *c = cm; *w = wm;
 }
 
-static void acc(orc_sketch *s, int slots, uint32_t c, float w) {
-  if (slots == 1) orc_bm_accumulate(s, c, w);
-  else orc_mg_accumulate(s, slots, c, w);
-}
-
 /* Sequential scan of edges [b, e) of u with stride st (self-loops skipped, rakLowmem.hxx:65). */
 static void scan_range(const orc_csr *g, uint32_t u, const uint32_t *vcom, int slots,
-                       int64_t b, int64_t e, int64_t st, orc_sketch *s) {
+                       int64_t b, int64_t e, int64_t st, orc_sketch *s, int gpu) {
   for (int64_t i = b; i < e; i += st) {
     uint32_t v = g->tgt[i];
     if (v == u) continue;
-    acc(s, slots, vcom[v], edge_w(g, i));
+    acc_rule(s, slots, vcom[v], edge_w(g, i), gpu);
   }
 }
 
 /* Fixed binary tree over lanes L[0..n): at each level lane s (< off) merges lane s+off. */
-static void tree_merge(orc_sketch *L, int n, int slots) {
+static void tree_merge(orc_sketch *L, int n, int slots, int gpu) {
   for (int off = n / 2; off >= 1; off /= 2)
-    for (int s = 0; s < off; ++s) orc_sketch_merge(&L[s], &L[s + off], slots);
+    for (int s = 0; s < off; ++s) merge_rule(&L[s], &L[s + off], slots, gpu);
+}
+
+/* A cleared sketch; Boyer-Moore under the GPU rules starts from the vertex's own label d with
+ * weight 0 (inc/rakLowmemCuda.hxx:41-43). */
+static void clear_rule(orc_sketch *s, int slots, int gpu, uint32_t d) {
+  orc_sketch_clear(s, slots);
+  if (gpu && slots == 1) s->k[0] = d;
 }
 
 static int group_size(const orc_layout *ly, int64_t deg) {
@@ -95,22 +128,23 @@ static int group_size(const orc_layout *ly, int64_t deg) {
 /* The split per-vertex sketch (documented in rak_oracle.h, orc_layout). */
 static void split_sketch(const orc_csr *g, const orc_opts *o, uint32_t u, const uint32_t *vcom,
                          orc_sketch *out) {
-  const int S = o->slots;
+  const int S = o->slots, gpu = o->gpu_rule;
+  const uint32_t d = vcom[u];
   const int64_t b = g->off[u], deg = g->off[u + 1] - g->off[u];
   const orc_layout *ly = &o->layout;
   orc_sketch L[32];
   if (deg <= ly->lane_max) {
-    orc_sketch_clear(out, S);
-    scan_range(g, u, vcom, S, b, b + deg, 1, out);
+    clear_rule(out, S, gpu, d);
+    scan_range(g, u, vcom, S, b, b + deg, 1, out, gpu);
     return;
   }
   if (deg <= ly->hub_min) {
     int G = group_size(ly, deg);
     for (int s = 0; s < G; ++s) {
-      orc_sketch_clear(&L[s], S);
-      scan_range(g, u, vcom, S, b + s, b + deg, G, &L[s]);
+      clear_rule(&L[s], S, gpu, d);
+      scan_range(g, u, vcom, S, b + s, b + deg, G, &L[s], gpu);
     }
-    tree_merge(L, G, S);
+    tree_merge(L, G, S, gpu);
     *out = L[0];
     return;
   }
@@ -119,17 +153,17 @@ static void split_sketch(const orc_csr *g, const orc_opts *o, uint32_t u, const 
   for (int64_t j = 0; j < nch; ++j) {
     int64_t cb = b + j * CH, ce = cb + CH < b + deg ? cb + CH : b + deg;
     for (int s = 0; s < 32; ++s) {
-      orc_sketch_clear(&L[s], S);
-      scan_range(g, u, vcom, S, cb + s, ce, 32, &L[s]);
+      clear_rule(&L[s], S, gpu, d);
+      scan_range(g, u, vcom, S, cb + s, ce, 32, &L[s], gpu);
     }
-    tree_merge(L, 32, S);
+    tree_merge(L, 32, S, gpu);
     C[j] = L[0];
   }
   for (int l = 0; l < 32; ++l) {
-    orc_sketch_clear(&L[l], S);
-    for (int64_t j = l; j < nch; j += 32) orc_sketch_merge(&L[l], &C[j], S);
+    clear_rule(&L[l], S, gpu, d);
+    for (int64_t j = l; j < nch; j += 32) merge_rule(&L[l], &C[j], S, gpu);
   }
-  tree_merge(L, 32, S);
+  tree_merge(L, 32, S, gpu);
   *out = L[0];
   free(C);
 }
@@ -153,11 +187,12 @@ void orc_choose(const orc_csr *g, const orc_opts *o, uint32_t u, const uint32_t 
   if (o->split) {
     split_sketch(g, o, u, vcom, &s);
   } else {
-    orc_sketch_clear(&s, o->slots);
-    scan_range(g, u, vcom, o->slots, g->off[u], g->off[u + 1], 1, &s);
+    clear_rule(&s, o->slots, o->gpu_rule, vcom[u]);
+    scan_range(g, u, vcom, o->slots, g->off[u], g->off[u + 1], 1, &s, o->gpu_rule);
     if (o->rescan && o->slots > 1) rescan(g, u, vcom, o->slots, &s);
   }
-  orc_sketch_choose(&s, o->slots, c, w);
+  if (o->gpu_rule) orc_sketch_choose_gpu(&s, o->slots, c, w);
+  else orc_sketch_choose(&s, o->slots, c, w);
 }
 
 static int is_pickless(const orc_opts *o, int l) { return o->pickless_step > 0 && l % o->pickless_step == 0; }
@@ -179,7 +214,9 @@ uint64_t orc_sync_step(const orc_csr *g, const orc_opts *o, int iteration,
     ++processed; edges += (uint64_t)deg;
     uint32_t d = vcom_prev[u], c; float w;
     orc_choose(g, o, (uint32_t)u, vcom_prev, &c, &w);
-    if (!(w > 0.0f) || c == d) continue;
+    /* CPU rule: w > 0; GPU rule: w != 0 for Misra-Gries, any candidate for Boyer-Moore */
+    const int weight_ok = o->gpu_rule ? (o->slots == 1 || w != 0.0f) : (w > 0.0f);
+    if (!weight_ok || c == d) continue;
     if (pl && c > d) continue;
     vcom_next[u] = c; ++changed;
     for (int64_t e = g->off[u]; e < g->off[u + 1]; ++e)
@@ -230,12 +267,12 @@ int orc_serial_run(const orc_csr *g, int slots, int rescan_on, double tolerance,
       uint32_t d = labels[u], c; float w;
       if (slots > 1) {
         for (int i = 0; i < slots; ++i) s.w[i] = 0.0f;
-        scan_range(g, (uint32_t)u, labels, slots, g->off[u], g->off[u + 1], 1, &s);
+        scan_range(g, (uint32_t)u, labels, slots, g->off[u], g->off[u + 1], 1, &s, 0);
         if (rescan_on) rescan(g, (uint32_t)u, labels, slots, &s);
         orc_sketch_choose(&s, slots, &c, &w);
       } else {
         orc_sketch bm; orc_sketch_clear(&bm, 1);
-        scan_range(g, (uint32_t)u, labels, 1, g->off[u], g->off[u + 1], 1, &bm);
+        scan_range(g, (uint32_t)u, labels, 1, g->off[u], g->off[u + 1], 1, &bm, 0);
         c = bm.k[0]; w = bm.w[0];
       }
       if (w > 0.0f && c != d) {

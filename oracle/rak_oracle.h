@@ -55,6 +55,9 @@ typedef struct orc_opts {
   int max_iterations;
   int pickless_step;      /* iterations l with l % step == 0 only move to smaller labels; 0 = never */
   int check_on_pickless;  /* 0: the tolerance test is skipped on pickless iterations */
+  int gpu_rule;           /* 0: the reference CPU sketch rules; 1: its GPU rules (first free slot,
+                             no clamp, tournament argmax, move if w != 0, Boyer-Moore from the
+                             vertex's own label) */
 } orc_opts;
 
 typedef struct orc_sketch {
@@ -68,6 +71,8 @@ void orc_mg_accumulate(orc_sketch *s, int slots, uint32_t c, float w);
 void orc_bm_accumulate(orc_sketch *s, uint32_t c, float w);
 void orc_sketch_merge(orc_sketch *a, const orc_sketch *b, int slots);
 void orc_sketch_choose(const orc_sketch *s, int slots, uint32_t *c, float *w);
+void orc_mg_accumulate_gpu(orc_sketch *s, int slots, uint32_t c, float w);
+void orc_sketch_choose_gpu(const orc_sketch *s, int slots, uint32_t *c, float *w);
 
 /* Best label of vertex u given a label snapshot vcom (before the move rule is applied). */
 void orc_choose(const orc_csr *g, const orc_opts *o, uint32_t u, const uint32_t *vcom,

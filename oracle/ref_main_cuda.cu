@@ -5,7 +5,8 @@
 // error, inc/_cuda.hxx:221-235, and sets device flags on every call, inc/rakLowmemCuda.hxx:570).
 // Built by oracle/Makefile into oracle/_ref/ref_lpa_cuda from the reference headers in place.
 //
-// usage: ref_lpa_cuda <graph.rakcsr> <slots: 1|8> <labels.out> [repeat] [tolerance] [max_iter]
+// usage: ref_lpa_cuda <graph.rakcsr> <slots: 1|8|0> <labels.out> [repeat] [tolerance] [max_iter]
+// (slots 0 runs the reference's ν-LPA, rakStaticCuda, inc/rakCuda.hxx:438-446, for comparison).
 // File format (written by tests and bench): "RAKCSR01", int64 n, int64 m, int32 has_weights,
 // int64 offsets[n+1], uint32 targets[m], float weights[m] (if has_weights).
 // Prints one JSON line: iterations, time_ms, marking/initialization ms, memory_gb.
@@ -80,7 +81,8 @@ int main(int argc, char **argv) {
   };
   if (slots == 1) { auto r = rakLowmemStaticCuda<1>(x, o); take(r); }
   else if (slots == 8) { auto r = rakLowmemStaticCuda<8>(x, o); take(r); }
-  else { fprintf(stderr, "slots must be 1 or 8\n"); return 2; }
+  else if (slots == 0) { auto r = rakStaticCuda(x, o); take(r); }  // ν-LPA (hashtable per vertex)
+  else { fprintf(stderr, "slots must be 0 (nu-LPA), 1 or 8\n"); return 2; }
   FILE *g = fopen(argv[3], "wb");
   if (!g || fwrite(labels.data(), 4, n, g) != size_t(n)) { perror("write"); return 2; }
   fclose(g);

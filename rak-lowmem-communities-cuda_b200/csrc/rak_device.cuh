@@ -16,10 +16,21 @@ struct Sketch {
   float w[S];
 };
 
-template <int S>
-__device__ __forceinline__ void sk_clear(Sketch<S> &s) {
+// The two rule sets of the reference: its CPU code's (inc/rakLowmem.hxx) and its GPU code's
+// (inc/sketchCuda.hxx, inc/rakLowmemCuda.hxx). They differ in which free slot a new key takes,
+// whether decrements clamp at zero, how the argmax breaks ties, the Boyer-Moore starting candidate
+// and the weight test of the move rule. The synchronous modes follow the CPU rules (bit-exact
+// against the reference CPU code); the asynchronous mode follows the GPU rules, the path it
+// replaces.
+enum : int { RULE_CPU = 1, RULE_GPU = 2 };
+
+// Cleared sketch. Boyer-Moore under the GPU rules starts from the vertex's own label d with weight
+// 0 (inc/rakLowmemCuda.hxx:41-43); otherwise keys start as NONE.
+template <int S, int RULE = RULE_CPU>
+__device__ __forceinline__ void sk_clear(Sketch<S> &s, uint32_t d = NONE) {
 #pragma unroll
   for (int i = 0; i < S; ++i) { s.k[i] = NONE; s.w[i] = 0.0f; }
+  if constexpr (S == 1 && RULE == RULE_GPU) s.k[0] = d;
 }
 
 // Weighted Misra-Gries accumulate with the reference CPU rule (inc/rakLowmem.hxx:63-89): add x to
@@ -47,32 +58,59 @@ __device__ __forceinline__ void mg_acc(Sketch<S> &s, uint32_t c, float x) {
   }
 }
 
-// Weighted Boyer-Moore vote (inc/rakLowmem.hxx:120-126, inc/rakLowmemCuda.hxx:49-51).
+// Weighted Misra-Gries accumulate with the reference GPU rule (inc/sketchCuda.hxx:73-108, one
+// thread's view of sketchAccumulateWarpCudU): add x to every slot keyed c; otherwise the FIRST slot
+// whose weight is exactly zero takes (c, x); otherwise every weight drops by x, with no clamp
+// (weights may go negative; a negative slot is not free).
+template <int S>
+__device__ __forceinline__ void mg_acc_gpu(Sketch<S> &s, uint32_t c, float x) {
+  bool hit = false;
+#pragma unroll
+  for (int i = 0; i < S; ++i)
+    if (s.k[i] == c) { s.w[i] = __fadd_rn(s.w[i], x); hit = true; }
+  if (hit) return;
+  int f = S;
+#pragma unroll
+  for (int i = S - 1; i >= 0; --i)
+    if (s.w[i] == 0.0f) f = i;
+  if (f < S) {
+#pragma unroll
+    for (int i = 0; i < S; ++i)
+      if (i == f) { s.k[i] = c; s.w[i] = x; }
+  } else {
+#pragma unroll
+    for (int i = 0; i < S; ++i) s.w[i] = __fsub_rn(s.w[i], x);
+  }
+}
+
+// Weighted Boyer-Moore vote (inc/rakLowmem.hxx:120-126, inc/rakLowmemCuda.hxx:49-51; the same
+// arithmetic under both rule sets).
 __device__ __forceinline__ void bm_acc(Sketch<1> &s, uint32_t c, float x) {
   if (c == s.k[0]) s.w[0] = __fadd_rn(s.w[0], x);
   else if (s.w[0] > x) s.w[0] = __fsub_rn(s.w[0], x);
   else { s.k[0] = c; s.w[0] = x; }
 }
 
-template <int S>
+template <int S, int RULE = RULE_CPU>
 __device__ __forceinline__ void sk_acc(Sketch<S> &s, uint32_t c, float x) {
   if constexpr (S == 1) bm_acc(s, c, x);
+  else if constexpr (RULE == RULE_GPU) mg_acc_gpu(s, c, x);
   else mg_acc(s, c, x);
 }
 
 // Merge by re-accumulating the other sketch's non-zero slots in slot order
 // (inc/sketchCuda.hxx:150-158).
-template <int S>
+template <int S, int RULE = RULE_CPU>
 __device__ __forceinline__ void sk_merge(Sketch<S> &a, const uint32_t (&bk)[S], const float (&bw)[S]) {
 #pragma unroll
   for (int j = 0; j < S; ++j)
-    if (bw[j] != 0.0f) sk_acc(a, bk[j], bw[j]);
+    if (bw[j] != 0.0f) sk_acc<S, RULE>(a, bk[j], bw[j]);
 }
 
 // Fixed binary tree over the G lanes of each aligned lane group (G a power of two <= 32):
 // at each level lane s < off merges the sketch of lane s+off. The group's result is in its
 // lane 0. Every lane of the warp must call this with the same G.
-template <int S>
+template <int S, int RULE = RULE_CPU>
 __device__ __forceinline__ void sk_tree(Sketch<S> &s, int G) {
   for (int off = G >> 1; off >= 1; off >>= 1) {
     uint32_t bk[S];
@@ -82,18 +120,35 @@ __device__ __forceinline__ void sk_tree(Sketch<S> &s, int G) {
       bk[j] = __shfl_down_sync(FULL, s.k[j], off, G);
       bw[j] = __shfl_down_sync(FULL, s.w[j], off, G);
     }
-    sk_merge(s, bk, bw);
+    sk_merge<S, RULE>(s, bk, bw);
   }
 }
 
-// Linear argmax with strict '>' from weight 0 (inc/rakLowmem.hxx:164-171).
-template <int S>
+// CPU rule: linear argmax with strict '>' from weight 0 (inc/rakLowmem.hxx:164-171).
+// GPU rule: the tournament of sketchMaxGroupReduceCudU (inc/sketchCuda.hxx:190-201) -- at each
+// level slot i takes slot i+S/2 only if strictly heavier -- whose winner may weigh <= 0.
+template <int S, int RULE = RULE_CPU>
 __device__ __forceinline__ void sk_choose(const Sketch<S> &s, uint32_t &c, float &w) {
-  c = NONE;
-  w = 0.0f;
+  if constexpr (RULE == RULE_GPU) {
+    uint32_t k[S];
+    float x[S];
 #pragma unroll
-  for (int i = 0; i < S; ++i)
-    if (s.w[i] > w) { w = s.w[i]; c = s.k[i]; }
+    for (int i = 0; i < S; ++i) { k[i] = s.k[i]; x[i] = s.w[i]; }
+#pragma unroll
+    for (int ds = S / 2; ds >= 1; ds /= 2) {
+#pragma unroll
+      for (int i = 0; i < ds; ++i)
+        if (x[i + ds] > x[i]) { k[i] = k[i + ds]; x[i] = x[i + ds]; }
+    }
+    c = k[0];
+    w = x[0];
+  } else {
+    c = NONE;
+    w = 0.0f;
+#pragma unroll
+    for (int i = 0; i < S; ++i)
+      if (s.w[i] > w) { w = s.w[i]; c = s.k[i]; }
+  }
 }
 
 // ---- run-wide state shared by all blocks of a persistent launch -------------------------

@@ -214,7 +214,7 @@ struct Events {
 };
 
 struct Resolved {
-  int slots, mode, rescan, pickless, check_on_pickless, iters, start, validate, modularity, repeat;
+  int slots, mode, rescan, pickless, check_on_pickless, iters, start, validate, modularity, repeat, rule;
   double tol;
   Layout ly;
 };
@@ -242,6 +242,13 @@ rak_status resolve(rak_ctx *ctx, const rak_options *o, Resolved *r) {
   if (r->iters < 0 || r->iters > 1024) { set_err(ctx, "max_iterations must be in [0, 1024]"); return RAK_ERR_INVALID_ARGUMENT; }
   r->tol = o->tolerance;
   if (!(r->tol >= 0)) { set_err(ctx, "tolerance must be >= 0"); return RAK_ERR_INVALID_ARGUMENT; }
+  r->rule = o->sketch_rule <= 0 ? (r->mode == RAK_MODE_ASYNC ? 2 : 1) : o->sketch_rule;
+  if (r->rule != 1 && r->rule != 2) { set_err(ctx, "sketch_rule must be -1, 0, 1 or 2"); return RAK_ERR_INVALID_ARGUMENT; }
+  if ((r->mode == RAK_MODE_ASYNC && r->rule != 2) || (r->mode == RAK_MODE_SYNC && r->rule != 1)) {
+    set_err(ctx, "RAK_MODE_ASYNC runs the GPU sketch rules and RAK_MODE_SYNC the CPU ones; "
+                 "RAK_MODE_SYNC_SPLIT runs either");
+    return RAK_ERR_UNSUPPORTED;
+  }
   r->start = o->start_iteration;
   r->validate = o->validate;
   r->modularity = o->compute_modularity;
@@ -477,7 +484,7 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
   a.sk_keys = b.skk.as<uint32_t>(); a.sk_wts = b.skw.as<float>();
   a.stats = b.stats.as<unsigned long long>(); a.rs = b.rs.p;
   a.iters = r.iters; a.start_iter = r.start; a.tolerance = r.tol; a.pickless_step = r.pickless;
-  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n); a.timeout_ns = 20LL * 1000 * 1000 * 1000;
+  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n); a.gpu_rule = r.rule == 2; a.timeout_ns = 20LL * 1000 * 1000 * 1000;
 
   // the kernel's module is loaded here, not inside the timed region
   if (r.iters > 0) RAK_TRY(ctx, rak::prepare_lpa(r.slots, r.mode, gr->off64, gr->wt == nullptr, false));
@@ -587,6 +594,7 @@ void rak_options_default(rak_options *o) {
   o->pickless_step = -1;
   o->check_on_pickless = -1;
   o->validate = 1;
+  o->sketch_rule = -1;
 }
 
 rak_status rak_ctx_create(int device, rak_ctx **out) {
@@ -790,7 +798,7 @@ rak_status rak_graph_step(rak_ctx *ctx, rak_graph *gr, const rak_options *o, int
   a.sk_keys = b.skk.as<uint32_t>(); a.sk_wts = b.skw.as<float>();
   a.stats = b.stats.as<unsigned long long>(); a.rs = b.rs.p;
   a.iters = 1; a.start_iter = iteration; a.tolerance = r.tol; a.pickless_step = r.pickless;
-  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n); a.timeout_ns = 20LL * 1000 * 1000 * 1000;
+  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n); a.gpu_rule = r.rule == 2; a.timeout_ns = 20LL * 1000 * 1000 * 1000;
   int grid = 0;
   RAK_TRY(ctx, rak::launch_lpa(a, r.slots, r.mode, gr->off64, st, &grid));
   unsigned long long s[rak::STATS_STRIDE] = {};
@@ -1011,7 +1019,7 @@ rak_status batch_enqueue(rak_ctx *ctx, rak_batch *b, const uint32_t *q, const Re
     a.giters = b->giters.as<int32_t>(); a.gchanged = b->gchanged.as<unsigned long long>();
     a.running = b->running.as<unsigned int>(); a.ngraphs = G; a.grid_cap = grid_cap;
     a.iters = r.iters; a.start_iter = r.start; a.tolerance = r.tol; a.pickless_step = r.pickless;
-    a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n); a.timeout_ns = 20LL * 1000 * 1000 * 1000;
+    a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n); a.gpu_rule = r.rule == 2; a.timeout_ns = 20LL * 1000 * 1000 * 1000;
     int grid = 0;
     RAK_TRY(ctx, rak::launch_lpa(a, r.slots, r.mode, true, st, &grid, true));
   }

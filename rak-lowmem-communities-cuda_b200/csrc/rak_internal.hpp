@@ -89,6 +89,7 @@ struct LpaArgs {
   int64_t ngraphs;
   int grid_cap;                 // at most this many blocks (0: as many as fit), to share the GPU
   int mark_test;                // neighbour marking reads a flag before storing it (mark_test_for)
+  int gpu_rule;                 // synchronous split mode: the reference GPU sketch rules (else CPU)
   int iters;
   int start_iter;
   double tolerance;

@@ -56,7 +56,7 @@ __device__ __forceinline__ float edge_w(const float *wt, int64_t e) {
 // the current batch's labels are gathered and accumulated. Positions past the end are given the
 // target u itself, which the self-loop rule skips. Labels are read with plain loads: they change
 // during the launch.
-template <int S, bool UNIT>
+template <int S, bool UNIT, int RULE>
 __device__ __forceinline__ void scan_range(Sketch<S> &sk, uint32_t u, int64_t e, int64_t ee, int st,
                                            const uint32_t *tgt, const float *wt, const uint32_t *vin,
                                            uint32_t base) {
@@ -84,7 +84,7 @@ __device__ __forceinline__ void scan_range(Sketch<S> &sk, uint32_t u, int64_t e,
     }
 #pragma unroll
     for (int j = 0; j < B; ++j)
-      if (t[j] != u) sk_acc(sk, c[j], w[j]);
+      if (t[j] != u) sk_acc<S, RULE>(sk, c[j], w[j]);
 #pragma unroll
     for (int j = 0; j < B; ++j) { t[j] = t2[j]; w[j] = w2[j]; }
     e = en;
@@ -225,9 +225,13 @@ __device__ __forceinline__ void count_move(const LpaArgs &a, uint32_t gi, int it
   if constexpr (BATCH) atomicAdd(a.gchanged + int64_t(it & 1) * a.ngraphs + gi, 1ull);
 }
 
+// CPU rule: w > 0 && c != d (inc/rakLowmem.hxx:203). GPU rule: the best weight is non-zero for
+// Misra-Gries (inc/rakLowmemCuda.hxx:306), any candidate for Boyer-Moore (:152). Both: on pickless
+// iterations no move to a larger label (:309, :153).
+template <int S, int RULE>
 __device__ __forceinline__ bool move_rule(float w, uint32_t c, uint32_t d, bool pickless) {
-  // inc/rakLowmem.hxx:203 (w>0 && c!=d) and inc/rakLowmemCuda.hxx:309 (pickless: no larger label)
-  return w > 0.0f && c != d && !(pickless && c > d);
+  const bool weight_ok = RULE == RULE_GPU ? (S == 1 || w != 0.0f) : w > 0.0f;
+  return weight_ok && c != d && !(pickless && c > d);
 }
 
 // Region 6: one lane per vertex. Items are collected into a per-warp queue of active vertices
@@ -253,7 +257,7 @@ __device__ __forceinline__ int lane_collect(const LpaArgs &a, const Regions &rg,
   return qn + __popc(m);
 }
 
-template <int S, int MODE, class O, bool UNIT, bool BATCH>
+template <int S, int MODE, class O, bool UNIT, bool BATCH, int RULE>
 __device__ __forceinline__ void lane_batch(const LpaArgs &a, const G_<O> &g, const uint32_t *q, int count,
                                            int it, bool pickless, const uint32_t *vin, uint32_t *vout,
                                            uint8_t *fin, uint8_t *fout, Counters &cnt) {
@@ -265,14 +269,14 @@ __device__ __forceinline__ void lane_batch(const LpaArgs &a, const G_<O> &g, con
   graph_of<BATCH>(a, u, gi, base);
   const int64_t eb = int64_t(__ldg(g.off + u)), ee = int64_t(__ldg(g.off + u + 1));
   Sketch<S> sk;
-  sk_clear(sk);
-  scan_range<S, UNIT>(sk, u, eb, ee, 1, g.tgt, g.wt, vin, base);
+  sk_clear<S, RULE>(sk, d);
+  scan_range<S, UNIT, RULE>(sk, u, eb, ee, 1, g.tgt, g.wt, vin, base);
   if constexpr (MODE == MODE_SYNC && S > 1)
     if (a.rescan) rescan_range<S, UNIT>(sk, u, eb, ee, g.tgt, g.wt, vin, base);
   uint32_t c;
   float w;
-  sk_choose(sk, c, w);
-  const bool moved = move_rule(w, c, d, pickless);
+  sk_choose<S, RULE>(sk, c, w);
+  const bool moved = move_rule<S, RULE>(w, c, d, pickless);
   cnt.processed += 1;
   cnt.edges += (unsigned long long)(ee - eb);
   if constexpr (MODE == MODE_ASYNC) {
@@ -290,7 +294,7 @@ __device__ __forceinline__ void lane_batch(const LpaArgs &a, const G_<O> &g, con
 }
 
 // Regions 1..5: aligned groups of G lanes per vertex.
-template <int S, int MODE, class O, bool UNIT, bool BATCH>
+template <int S, int MODE, class O, bool UNIT, bool BATCH, int RULE>
 __device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, const G_<O> &g, int r, int64_t local,
                                            int it, bool pickless, const uint32_t *vin, uint32_t *vout,
                                            uint8_t *fin, uint8_t *fout, Counters &cnt) {
@@ -308,17 +312,17 @@ __device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, 
     if (active) { eb = int64_t(__ldg(g.off + u)); ee = int64_t(__ldg(g.off + u + 1)); }
   }
   Sketch<S> sk;
-  sk_clear(sk);
+  sk_clear<S, RULE>(sk, d);
   if constexpr (MODE == MODE_SYNC) {
     if (active) exact_group_scan<S, UNIT>(sk, u, eb, ee, G, grp, s, S > 1 && a.rescan, g.tgt, g.wt, vin, base);
   } else {
-    if (active) scan_range<S, UNIT>(sk, u, eb + s, ee, G, g.tgt, g.wt, vin, base);
-    sk_tree(sk, G);
+    if (active) scan_range<S, UNIT, RULE>(sk, u, eb + s, ee, G, g.tgt, g.wt, vin, base);
+    sk_tree<S, RULE>(sk, G);
   }
   uint32_t c;
   float w;
-  sk_choose(sk, c, w);
-  bool moved = active && move_rule(w, c, d, pickless);
+  sk_choose<S, RULE>(sk, c, w);
+  bool moved = active && move_rule<S, RULE>(w, c, d, pickless);
   moved = __shfl_sync(FULL, moved, grp * G);
   if (s == 0 && valid) {
     if (active) { cnt.processed += 1; cnt.edges += (unsigned long long)(ee - eb); }
@@ -338,7 +342,7 @@ __device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, 
 // warp builds a partial sketch (lane-strided, tree-merged), stores it, and the last chunk to
 // arrive merges all partial sketches in a fixed order and makes the move; its neighbours are
 // marked in a second phase after the iteration's barrier.
-template <int S, int MODE, class O, bool UNIT, bool BATCH>
+template <int S, int MODE, class O, bool UNIT, bool BATCH, int RULE>
 __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, const G_<O> &g, int64_t local, int it, bool pickless,
                                          const uint32_t *vin, uint32_t *vout, uint8_t *fin, uint8_t *fout,
                                          Counters &cnt) {
@@ -354,12 +358,12 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
     const uint32_t d = vin[u];
     const bool active = fin[u] != 0 && !gfin;
     Sketch<S> sk;
-    sk_clear(sk);
+    sk_clear<S, RULE>(sk, d);
     if (active) exact_group_scan<S, UNIT>(sk, u, eb, ee, 32, 0, lane, S > 1 && a.rescan, g.tgt, g.wt, vin, base);
     uint32_t c;
     float w;
-    sk_choose(sk, c, w);
-    const bool moved = active && move_rule(w, c, d, pickless);
+    sk_choose<S, RULE>(sk, c, w);
+    const bool moved = active && move_rule<S, RULE>(w, c, d, pickless);
     if (lane == 0) {
       vout[u] = moved ? c : d;
       if (active) { cnt.processed += 1; cnt.edges += (unsigned long long)(ee - eb); }
@@ -394,11 +398,13 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
       }
       active = __shfl_sync(FULL, dec, 0) != 0;
     }
+    // Boyer-Moore under the GPU rules starts every partial vote from u's label
+    const uint32_t d0 = (S == 1 && RULE == RULE_GPU) ? vin[u] : NONE;
     Sketch<S> sk;
-    sk_clear(sk);
+    sk_clear<S, RULE>(sk, d0);
     const int64_t cb = eb + j * a.hub_chunk, ce = cb + a.hub_chunk < ee ? cb + a.hub_chunk : ee;
-    if (active) scan_range<S, UNIT>(sk, u, cb + lane, ce, 32, g.tgt, g.wt, vin, base);
-    sk_tree(sk, 32);
+    if (active) scan_range<S, UNIT, RULE>(sk, u, cb + lane, ce, 32, g.tgt, g.wt, vin, base);
+    sk_tree<S, RULE>(sk, 32);
     unsigned int last = 0;
     if (lane == 0) {
       if (active) {
@@ -422,7 +428,7 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
       return;
     }
     Sketch<S> acc;
-    sk_clear(acc);
+    sk_clear<S, RULE>(acc, d0);
     for (int64_t jj = lane; jj < nch; jj += 32) {
       uint32_t bk[S];
       float bw[S];
@@ -431,14 +437,14 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
         bk[i] = __ldcg(a.sk_keys + (first + jj) * S + i);
         bw[i] = __ldcg(a.sk_wts + (first + jj) * S + i);
       }
-      sk_merge(acc, bk, bw);
+      sk_merge<S, RULE>(acc, bk, bw);
     }
-    sk_tree(acc, 32);
+    sk_tree<S, RULE>(acc, 32);
     if (lane == 0) {
       uint32_t c;
       float w;
-      sk_choose(acc, c, w);
-      const bool moved = move_rule(w, c, d, pickless);
+      sk_choose<S, RULE>(acc, c, w);
+      const bool moved = move_rule<S, RULE>(w, c, d, pickless);
       cnt.processed += 1;
       if constexpr (MODE == MODE_ASYNC) {
         if (moved) vout[u] = c;
@@ -455,6 +461,18 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
     }
   }
 }
+
+// The rule set of a work item: the asynchronous mode follows the reference GPU rules, the exact
+// synchronous mode the CPU rules, and the synchronous split mode either, per launch (a.gpu_rule).
+#define RAK_BY_RULE(F, ARGS)                                                            \
+  do {                                                                                 \
+    if constexpr (MODE == MODE_SPLIT) {                                                \
+      if (a.gpu_rule) F<S, MODE, O, UNIT, BATCH, RULE_GPU> ARGS;                       \
+      else F<S, MODE, O, UNIT, BATCH, RULE_CPU> ARGS;                                  \
+    } else {                                                                           \
+      F<S, MODE, O, UNIT, BATCH, MODE == MODE_ASYNC ? RULE_GPU : RULE_CPU> ARGS;       \
+    }                                                                                  \
+  } while (0)
 
 template <int S, int MODE, class O, bool UNIT, bool BATCH>
 __global__ void __launch_bounds__(256, RAK_MIN_BLOCKS) lpa_run(const LpaArgs a) {
@@ -494,19 +512,19 @@ __global__ void __launch_bounds__(256, RAK_MIN_BLOCKS) lpa_run(const LpaArgs a) 
       if (r == REG_LANE) {
         qn = lane_collect<S, MODE, O, UNIT, BATCH>(a, rg, local, vin, vout, fin, q, qn);
         if (qn >= 32) {
-          lane_batch<S, MODE, O, UNIT, BATCH>(a, g, q, 32, it, pickless, vin, vout, fin, fout, cnt);
+          RAK_BY_RULE(lane_batch, (a, g, q, 32, it, pickless, vin, vout, fin, fout, cnt));
           __syncwarp();
           if (lane < qn - 32) q[lane] = q[32 + lane];
           __syncwarp();
           qn -= 32;
         }
       } else if (r == REG_HUB) {
-        hub_item<S, MODE, O, UNIT, BATCH>(a, rg, g, local, it, pickless, vin, vout, fin, fout, cnt);
+        RAK_BY_RULE(hub_item, (a, rg, g, local, it, pickless, vin, vout, fin, fout, cnt));
       } else {
-        group_item<S, MODE, O, UNIT, BATCH>(a, rg, g, r, local, it, pickless, vin, vout, fin, fout, cnt);
+        RAK_BY_RULE(group_item, (a, rg, g, r, local, it, pickless, vin, vout, fin, fout, cnt));
       }
     }
-    if (qn > 0) lane_batch<S, MODE, O, UNIT, BATCH>(a, g, q, qn, it, pickless, vin, vout, fin, fout, cnt);
+    if (qn > 0) RAK_BY_RULE(lane_batch, (a, g, q, qn, it, pickless, vin, vout, fin, fout, cnt));
     __syncwarp();
     const unsigned long long ch = warp_sum((unsigned long long)cnt.changed);
     const unsigned long long ed = warp_sum(cnt.edges);

@@ -246,6 +246,7 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   a.pickless_step = o->pickless_step < 0 ? (mode == RAK_MODE_ASYNC ? 8 : 0) : o->pickless_step;
   a.check_on_pickless = o->check_on_pickless < 0 ? (mode == RAK_MODE_ASYNC ? 0 : 1) : (o->check_on_pickless ? 1 : 0);
   a.rescan = rescan;
+  a.gpu_rule = mode == RAK_MODE_SYNC_SPLIT && o->sketch_rule == 2;  // ASYNC: GPU rules, SYNC: CPU rules, fixed
   a.timeout_ns = 20LL * 1000 * 1000 * 1000;
   if (iters > 0) {
     int grid = 0;

@@ -43,7 +43,8 @@ class rak_options(C.Structure):
                 ("pickless_step", C.c_int32), ("check_on_pickless", C.c_int32), ("lane_max", C.c_int32),
                 ("hub_min", C.c_int32), ("hub_chunk", C.c_int32), ("validate", C.c_int32),
                 ("compute_modularity", C.c_int32), ("start_iteration", C.c_int32),
-                ("initial_flags", C.c_void_p), ("reserved", C.c_int64 * 8)]
+                ("initial_flags", C.c_void_p), ("sketch_rule", C.c_int32), ("reserved32", C.c_int32),
+                ("reserved", C.c_int64 * 7)]
 
 
 class rak_result(C.Structure):

@@ -76,3 +76,26 @@ def test_known_answer_streams():
     assert b.choose() == (4, 1.0)
     b.add(4, 2.0).add(9, 1.0)
     assert b.choose() == (4, 2.0)
+
+
+def test_gpu_rule_known_answers():
+    """The reference GPU sketch rules (inc/sketchCuda.hxx): a new key takes the FIRST free slot,
+    a full sketch decrements without clamping (negative slots are not free), and the argmax is a
+    tournament whose winner may weigh <= 0."""
+    s = orc.Sketch(4, gpu_rule=True).add(7, 1.0).add(8, 1.0)
+    assert s.slots_list()[:2] == [(7, 1.0), (8, 1.0)]              # slots 0, 1 (CPU rule: 3, 2)
+    c = orc.Sketch(4).add(7, 1.0).add(8, 1.0)
+    assert c.slots_list()[2:] == [(8, 1.0), (7, 1.0)]
+    s = orc.Sketch(2, gpu_rule=True).add(1, 1.0).add(2, 3.0).add(3, 2.0)   # full: both drop by 2
+    assert s.slots_list() == [(1, -1.0), (2, 1.0)]
+    s.add(4, 5.0)                                                   # still no free slot: drop again
+    assert s.slots_list() == [(1, -6.0), (2, -4.0)]
+    assert s.choose() == (2, -4.0)                                  # winner may be negative
+    t = orc.Sketch(4, gpu_rule=True).add(1, 1.0).add(2, 2.0).add(3, 2.0).add(4, 1.0)
+    assert t.choose() == (3, 2.0)                                   # tournament: slot 2 beats slot 0,
+    u = orc.Sketch(4).add(1, 1.0).add(2, 2.0).add(3, 2.0).add(4, 1.0)   # slot 1 never beats it
+    assert u.choose()[1] == 2.0
+    z = orc.Sketch(2, gpu_rule=True).add(5, 2.0).add(6, 2.0).add(7, 2.0)   # exact zero frees a slot
+    assert z.slots_list() == [(5, 0.0), (6, 0.0)]
+    z.add(8, 1.0)
+    assert z.slots_list() == [(8, 1.0), (6, 0.0)]

@@ -88,11 +88,11 @@ def degree_ladder():
     return g
 
 
-def check_sync(ctx, g, slots, rescan, split):
-    o = orc.make_opts(slots=slots, rescan=rescan, split=split, layout=orc.DEFAULT_LAYOUT)
+def check_sync(ctx, g, slots, rescan, split, gpu_rule=0):
+    o = orc.make_opts(slots=slots, rescan=rescan, split=split, layout=orc.DEFAULT_LAYOUT, gpu_rule=gpu_rule)
     ref, it, edges = orc.sync_run(orc.Graph.of(g), o)
     mode = rl.MODE_SYNC_SPLIT if split else rl.MODE_SYNC
-    lab, res = ctx.lowmem(g, mode=mode, slots=slots, rescan=rescan)
+    lab, res = ctx.lowmem(g, mode=mode, slots=slots, rescan=rescan, sketch_rule=2 if gpu_rule else 1)
     assert res.iterations == it
     np.testing.assert_array_equal(lab, ref)
     assert res.traversed_edges == edges
@@ -104,16 +104,18 @@ def test_multigraph_sync_exact(ctx, slots, rescan):
 
 
 @pytest.mark.parametrize("slots", [8, 2, 1])
-def test_multigraph_sync_split(ctx, slots):
-    check_sync(ctx, multigraph(), slots, 0, split=1)
+@pytest.mark.parametrize("gpu_rule", [0, 1])
+def test_multigraph_sync_split(ctx, slots, gpu_rule):
+    check_sync(ctx, multigraph(), slots, 0, split=1, gpu_rule=gpu_rule)
 
 
 @pytest.mark.parametrize("slots", [8, 1])
-def test_degree_boundaries_sync_split_default_layout(ctx, slots):
+@pytest.mark.parametrize("gpu_rule", [0, 1])
+def test_degree_boundaries_sync_split_default_layout(ctx, slots, gpu_rule):
     g = degree_ladder()
     summary = rl.plan_summary(g)
     assert summary[0][6] >= 2                                  # split vertices exist at the default layout
-    check_sync(ctx, g, slots, 0, split=1)
+    check_sync(ctx, g, slots, 0, split=1, gpu_rule=gpu_rule)
 
 
 def test_degree_boundaries_sync_exact(ctx):

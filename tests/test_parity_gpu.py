@@ -244,3 +244,28 @@ def test_device_csr_and_resident_runs(ctx):
     assert r2.time_ms > 0 and rg.device_bytes() > 0
     assert ctx.modularity(csr, out2) == pytest.approx(orc.modularity(orc.Graph.of(g), host), rel=1e-9)
     rg.close()
+
+
+@pytest.mark.parametrize("name", sorted(GRAPHS))
+@pytest.mark.parametrize("slots", [8, 4, 1])
+@pytest.mark.parametrize("layout", [SMALL_LAYOUT, TINY_LAYOUT, None])
+def test_sync_split_gpu_rule_matches_oracle(ctx, name, slots, layout):
+    """The reference GPU sketch rules (the asynchronous mode's) checked bit for bit: the split
+    mode run with sketch_rule 2 against the oracle's restatement of those rules."""
+    g = GRAPHS[name]
+    lab, res = ctx.lowmem(g, mode=rl.MODE_SYNC_SPLIT, slots=slots, sketch_rule=2, **(layout or {}))
+    ref, it, edges = orc.sync_run(orc.Graph.of(g), ocfg(slots, 0, split=1, layout=layout, gpu_rule=1))
+    assert res.iterations == it
+    np.testing.assert_array_equal(lab, ref)
+    assert res.traversed_edges == edges
+
+
+def test_sketch_rule_mode_combinations(ctx):
+    g = GRAPHS["rmat10"]
+    for mode, rule in ((rl.MODE_ASYNC, 1), (rl.MODE_SYNC, 2)):
+        with pytest.raises(rl.RakError) as e:
+            ctx.lowmem(g, mode=mode, sketch_rule=rule)
+        assert e.value.status == 7
+    with pytest.raises(rl.RakError) as e:
+        ctx.lowmem(g, sketch_rule=3)
+    assert e.value.status == 1

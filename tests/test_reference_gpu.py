@@ -62,4 +62,6 @@ def test_against_reference_gpu(ctx, slots):
         print("REFGPU " + json.dumps(rec))
         assert lab.max() < g.n
         tol = 0.005 if slots > 1 else 0.05
-        assert q >= q_ref - tol * abs(q_ref), rec
+        # plus 1e-3 absolute: on unpermuted R-MAT both implementations can end in one giant
+        # community (Q ~ 1e-5), where a relative tolerance compares noise
+        assert q >= q_ref - tol * abs(q_ref) - 1e-3, rec
