@@ -564,7 +564,8 @@ def main():
     peak, peak_kind = peaks()
     traffic = traffic_for(args.workload)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": f"{peak_kind} HBM copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
+                "peak_source": ("measured HBM copy bandwidth (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                                else "fallback HBM copy bandwidth 6650 GB/s (MEASURED_PEAKS.json absent)"),
                 "kernel": "rak::lpa_run (persistent, all iterations in one launch)",
                 "algorithmic_bytes_per_launch": bytes_per_launch, "launch_ms": loop_s * 1e3,
                 "traffic": traffic["bytes_per_launch"] if traffic else None}

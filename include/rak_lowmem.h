@@ -95,9 +95,14 @@ typedef struct rak_options {
   int32_t sketch_rule;        /* -1 or 0: mode default; 1: the reference CPU sketch rules (last free
                                  slot, clamped decrement, linear argmax, move if w > 0); 2: its GPU
                                  rules (first free slot, unclamped, tournament argmax, move if
-                                 w != 0, Boyer-Moore from the own label). ASYNC uses 2, SYNC 1,
-                                 SYNC_SPLIT either [1] */
-  int32_t reserved32;
+                                 w != 0, Boyer-Moore from the own label). SYNC runs 1 only;
+                                 ASYNC and SYNC_SPLIT run either [1] */
+  int32_t label_order;        /* -1 or 0: mode default; 1: labels are vertex ids; 2: labels are
+                                 positions in the reference GPU path's vertex order (degree
+                                 partition, inc/rakLowmemCuda.hxx:505-519, 563), which its pickless
+                                 rule compares; results are vertex ids either way. ASYNC: 2 [2];
+                                 SYNC modes: 1 only. Graph steps, batches, the server and the
+                                 no-alloc entry label by id and refuse 2 */
   int64_t reserved[7];
 } rak_options;
 
@@ -321,7 +326,8 @@ rak_status rak_server_destroy(rak_server *s);
  * The first call on a device looks the array up on that device (make it before any stream
  * capture). All calls share the array and it keeps the last call's contents; each call clears
  * what must start at zero, and calls that overlap on the GPU race on it. Times in res are host
- * wall-clock (no CUDA events are created). */
+ * wall-clock (no CUDA events are created). Labels are vertex ids in every mode: label_order 2
+ * returns RAK_ERR_UNSUPPORTED. */
 rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const rak_csr *g, const uint32_t *q,
                                    const rak_options *o, uint32_t *membership, rak_result *res);
 
@@ -350,6 +356,11 @@ rak_status rak_gen_rmat(int scale, double edge_factor, double a, double b, doubl
 rak_status rak_gen_rmat_device(rak_ctx *ctx, int scale, double edge_factor, double a, double b, double c,
                                uint64_t seed, float w_lo, float w_hi, int32_t offset_bits, rak_csr *out);
 rak_status rak_device_csr_free(rak_csr *g);
+/* The vertex order the reference's GPU path works in (inc/rakLowmemCuda.hxx:505-519, 563: vertex
+ * ids partitioned by degree < 4, then the rest by degree < 128, with libstdc++'s std::partition
+ * exchange), whose positions name the labels of asynchronous runs (rak_options.label_order).
+ * g device-located; ks: device, n entries (ks[i] = i-th vertex). */
+rak_status rak_reference_vertex_order(rak_ctx *ctx, const rak_csr *g, uint32_t *ks);
 /* Copies a device-located CSR into newly allocated host arrays (offsets widened to 64 bits); free
  * them with rak_host_csr_free. */
 rak_status rak_device_csr_to_host(const rak_csr *g, rak_host_csr *out);

@@ -198,6 +198,7 @@ def ref_cpu():
         _sig(_ref, "ref_modularity", C.c_double, C.c_int64, P, P, P, P)
         _sig(_ref, "ref_sync_step", C.c_int64, C.c_int64, P, P, P, C.c_int, C.c_int, C.c_int, P, P, P, P)
         _sig(_ref, "ref_sketch_stream", C.c_int, C.c_int, C.c_int64, P, P, P, P)
+        _sig(_ref, "ref_vertex_order", None, C.c_int64, P, P)
         _sig(_ref, "ref_read_mtx", C.c_int, C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_int64),
              C.POINTER(C.c_int64), P, P, P)
     return _ref
@@ -214,6 +215,14 @@ def ref_read_mtx(path, weighted=False, symmetrize=True):
     ref_cpu().ref_read_mtx(str(path).encode(), int(weighted), int(symmetrize), C.byref(n), C.byref(m),
                            off.ctypes.data, tgt.ctypes.data, wt.ctypes.data)
     return off, tgt[:m.value], (wt[:m.value] if weighted else None)
+
+
+def ref_vertex_order(g):
+    """The reference GPU entry's vertex order (std::partition by degree < 4, then < 128)."""
+    g = Graph.of(g)
+    ks = np.empty(g.n, np.uint32)
+    ref_cpu().ref_vertex_order(g.n, g.offsets.ctypes.data, ks.ctypes.data)
+    return ks
 
 
 def ref_sketch_stream(slots, comm, wts):

@@ -13,7 +13,9 @@
 #define OPENMP 1
 #include <cstdint>
 #include <cstdio>
+#include <algorithm>
 #include <array>
+#include <numeric>
 #include <vector>
 #include <omp.h>
 #include "_main.hxx"
@@ -225,6 +227,21 @@ int ref_read_mtx(const char *path, int weighted, int symmetrize, int64_t *n, int
     off[u] = e;
   }
   return 0;
+}
+
+// The vertex order of the reference's GPU entry (rakLowmemPartitionVerticesCudaU,
+// inc/rakLowmemCuda.hxx:505-519, on vertexKeys(x)): keys in order, std::partition by degree < 4,
+// then the remainder by degree < 128. That header needs the CUDA toolchain, so the two calls are
+// restated here with the same predicates on the same standard library; 0-based ids (the
+// reference's keys are these + 1, which does not change the order).
+void ref_vertex_order(int64_t n, const int64_t *off, uint32_t *ks) {
+  vector<uint32_t> k(static_cast<size_t>(n));
+  std::iota(k.begin(), k.end(), 0u);
+  auto fl = [&](uint32_t v) { return off[v + 1] - off[v] < 4; };
+  auto fm = [&](uint32_t v) { return off[v + 1] - off[v] < 128; };
+  auto il = std::partition(k.begin(), k.end(), fl);
+  std::partition(il, k.end(), fm);
+  std::copy(k.begin(), k.end(), ks);
 }
 
 }  // extern "C"

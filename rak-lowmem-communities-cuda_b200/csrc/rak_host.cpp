@@ -141,6 +141,9 @@ struct rak_graph {
   rak_host_detail::RunBufs bufs;  // run buffers reused across runs
   // plan storage (order and split-vertex tables) and its build space, grown only when too small
   rak_host_detail::DevBuf p_order, p_hub_first, p_chunk_hub, p_keys, p_keys2, p_vids, p_hist, p_temp, p_deg;
+  // the reference GPU path's vertex order (asynchronous runs name labels by position in it)
+  rak_host_detail::DevBuf ref_ks, ref_pos;
+  bool ref_ready = false;
 };
 
 struct rak_batch {
@@ -214,7 +217,7 @@ struct Events {
 };
 
 struct Resolved {
-  int slots, mode, rescan, pickless, check_on_pickless, iters, start, validate, modularity, repeat, rule;
+  int slots, mode, rescan, pickless, check_on_pickless, iters, start, validate, modularity, repeat, rule, order;
   double tol;
   Layout ly;
 };
@@ -242,11 +245,18 @@ rak_status resolve(rak_ctx *ctx, const rak_options *o, Resolved *r) {
   if (r->iters < 0 || r->iters > 1024) { set_err(ctx, "max_iterations must be in [0, 1024]"); return RAK_ERR_INVALID_ARGUMENT; }
   r->tol = o->tolerance;
   if (!(r->tol >= 0)) { set_err(ctx, "tolerance must be >= 0"); return RAK_ERR_INVALID_ARGUMENT; }
-  r->rule = o->sketch_rule <= 0 ? (r->mode == RAK_MODE_ASYNC ? 2 : 1) : o->sketch_rule;
+  // every mode defaults to the CPU rules: the GPU rules' unclamped decrement lets R-MAT-like graphs
+  // collapse into one community (as the reference GPU path does); they stay selectable
+  r->rule = o->sketch_rule <= 0 ? 1 : o->sketch_rule;
   if (r->rule != 1 && r->rule != 2) { set_err(ctx, "sketch_rule must be -1, 0, 1 or 2"); return RAK_ERR_INVALID_ARGUMENT; }
-  if ((r->mode == RAK_MODE_ASYNC && r->rule != 2) || (r->mode == RAK_MODE_SYNC && r->rule != 1)) {
-    set_err(ctx, "RAK_MODE_ASYNC runs the GPU sketch rules and RAK_MODE_SYNC the CPU ones; "
-                 "RAK_MODE_SYNC_SPLIT runs either");
+  if (r->mode == RAK_MODE_SYNC && r->rule != 1) {
+    set_err(ctx, "RAK_MODE_SYNC runs the CPU sketch rules (bit-exact with the reference CPU code)");
+    return RAK_ERR_UNSUPPORTED;
+  }
+  r->order = o->label_order <= 0 ? (r->mode == RAK_MODE_ASYNC ? 2 : 1) : o->label_order;
+  if (r->order != 1 && r->order != 2) { set_err(ctx, "label_order must be -1, 0, 1 or 2"); return RAK_ERR_INVALID_ARGUMENT; }
+  if (r->order == 2 && r->mode != RAK_MODE_ASYNC) {
+    set_err(ctx, "the synchronous modes label vertices by id (bit-exact with the reference CPU code)");
     return RAK_ERR_UNSUPPORTED;
   }
   r->start = o->start_iteration;
@@ -261,6 +271,17 @@ rak_status resolve(rak_ctx *ctx, const rak_options *o, Resolved *r) {
             (long long)rak::MAX_LANE_MAX);
     return RAK_ERR_INVALID_ARGUMENT;
   }
+  return RAK_OK;
+}
+
+// Entry points whose labels are always vertex ids (graph steps, batches, the server): an explicit
+// request for the reference label order is refused rather than ignored.
+rak_status ids_only(rak_ctx *ctx, const rak_options *o, Resolved *r) {
+  if (o && o->label_order == 2) {
+    set_err(ctx, "label_order 2 applies to single-graph runs (rak_lowmem_cuda, rak_graph_run)");
+    return RAK_ERR_UNSUPPORTED;
+  }
+  r->order = 1;
   return RAK_OK;
 }
 
@@ -488,6 +509,20 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
 
   // the kernel's module is loaded here, not inside the timed region
   if (r.iters > 0) RAK_TRY(ctx, rak::prepare_lpa(r.slots, r.mode, gr->off64, gr->wt == nullptr, false));
+  // Labels as positions in the reference GPU path's vertex order (inc/rakLowmemCuda.hxx:563,
+  // 591-592), so that its pickless rule compares the same label order; turned back into vertex ids
+  // after the run. The order depends on degrees only: built once per graph.
+  const bool ref_labels = r.order == 2 && n > 0;
+  if (ref_labels && !gr->ref_ready) {
+    DevBuf scratch;
+    RAK_TRY(ctx, ensure(gr->ref_ks, size_t(n) * 4));
+    RAK_TRY(ctx, ensure(gr->ref_pos, size_t(n) * 4));
+    RAK_TRY(ctx, scratch.alloc(rak::ref_order_scratch_bytes(n), nullptr));
+    RAK_TRY(ctx, rak::ref_order(gr->off, gr->off64, n, gr->ref_ks.as<uint32_t>(), gr->ref_pos.as<uint32_t>(), scratch.p, st));
+    RAK_TRY(ctx, cudaStreamSynchronize(st));
+    gr->ref_ready = true;
+  }
+  if (ref_labels && tr) tr->add(gr->ref_ks.bytes + gr->ref_pos.bytes);
   Events ev;
   float t_init = 0, t_mark = 0, t_all = 0, t_loop = 0;
   rak::RunStateHost hs{};
@@ -499,7 +534,8 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
     RAK_TRY(ctx, cudaMemsetAsync(b.stats.p, 0, b.stats.bytes, st));
     RAK_TRY(ctx, cudaMemsetAsync(b.rs.p, 0, b.rs.bytes, st));
     cudaEventRecord(ev.e[0], st);
-    RAK_TRY(ctx, rak::launch_init(vcom0, sync ? a.vcom1 : nullptr, q, n, st));
+    if (ref_labels) RAK_TRY(ctx, rak::launch_init_mapped(vcom0, q, gr->ref_pos.as<uint32_t>(), n, st));
+    else RAK_TRY(ctx, rak::launch_init(vcom0, sync ? a.vcom1 : nullptr, q, n, st));
     cudaEventRecord(ev.e[1], st);
     RAK_TRY(ctx, rak::launch_init_flags(a.aff0, sync ? a.aff1 : nullptr, flags, n, st));
     cudaEventRecord(ev.e[2], st);
@@ -523,6 +559,7 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
   }
   const int done = r.iters > 0 ? int(hs.iterations) : 0;
   if (sync && (done & 1)) RAK_TRY(ctx, cudaMemcpyAsync(vcom0, a.vcom1, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
+  if (ref_labels) RAK_TRY(ctx, rak::launch_labels_to_ids(vcom0, gr->ref_ks.as<uint32_t>(), n, st));
   RAK_TRY(ctx, cudaStreamSynchronize(st));
   if (res) {
     res->iterations = done;
@@ -595,6 +632,7 @@ void rak_options_default(rak_options *o) {
   o->check_on_pickless = -1;
   o->validate = 1;
   o->sketch_rule = -1;
+  o->label_order = -1;
 }
 
 rak_status rak_ctx_create(int device, rak_ctx **out) {
@@ -762,6 +800,7 @@ rak_status rak_graph_step(rak_ctx *ctx, rak_graph *gr, const rak_options *o, int
   if (!ctx || !gr || !vcom_prev || !aff_prev || !vcom_next || !aff_next) return RAK_ERR_INVALID_ARGUMENT;
   Resolved r;
   RAK_CHECK(resolve(ctx, o, &r));
+  RAK_CHECK(ids_only(ctx, o, &r));
   RAK_TRY(ctx, cudaSetDevice(ctx->device));
   if (!same_layout(gr->ly, r.ly)) RAK_CHECK(build_plan(ctx, gr, r.ly, nullptr));
   cudaStream_t st = ctx->stream;
@@ -909,6 +948,20 @@ rak_status rak_device_csr_to_host(const rak_csr *g, rak_host_csr *out) {
   return RAK_OK;
 }
 
+rak_status rak_reference_vertex_order(rak_ctx *ctx, const rak_csr *g, uint32_t *ks) {
+  cudaGetLastError();  // drop a stale error left by an unrelated failed call
+  if (!ctx || !g || !ks || g->location != RAK_DEVICE) return RAK_ERR_INVALID_ARGUMENT;
+  RAK_CHECK(check_csr_shape(ctx, g));
+  RAK_TRY(ctx, cudaSetDevice(ctx->device));
+  if (g->n == 0) return RAK_OK;
+  DevBuf pos, scratch;
+  RAK_TRY(ctx, pos.alloc(size_t(g->n) * 4, nullptr));
+  RAK_TRY(ctx, scratch.alloc(rak::ref_order_scratch_bytes(g->n), nullptr));
+  RAK_TRY(ctx, rak::ref_order(g->offsets, g->offset_bits == 64, g->n, ks, pos.as<uint32_t>(), scratch.p, ctx->stream));
+  RAK_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return RAK_OK;
+}
+
 rak_status rak_device_csr_free(rak_csr *g) {
   if (!g || g->location != RAK_DEVICE) return RAK_ERR_INVALID_ARGUMENT;
   cudaFree(const_cast<void *>(g->offsets));
@@ -1041,6 +1094,7 @@ rak_status rak_batch_create(rak_ctx *ctx, const rak_batch_csr *bc, const rak_opt
   if (bc->graphs < 0 || !bc->graph_offsets) { set_err(ctx, "bad graph count or offsets"); return RAK_ERR_INVALID_ARGUMENT; }
   Resolved r;
   RAK_CHECK(resolve(ctx, o, &r));
+  RAK_CHECK(ids_only(ctx, o, &r));
   RAK_TRY(ctx, cudaSetDevice(ctx->device));
   rak_csr c{};
   c.n = bc->n; c.m = bc->m; c.offset_bits = 64; c.location = bc->location;
@@ -1106,6 +1160,7 @@ rak_status rak_batch_launch(rak_ctx *ctx, rak_batch *b, const uint32_t *q, const
   if (!ctx || !b || !membership) return RAK_ERR_INVALID_ARGUMENT;
   Resolved r;
   RAK_CHECK(resolve(ctx, o, &r));
+  RAK_CHECK(ids_only(ctx, o, &r));
   RAK_TRY(ctx, cudaSetDevice(ctx->device));
   RAK_CHECK(batch_prepare(ctx, b, r));
   return batch_enqueue(ctx, b, q, r, membership);
@@ -1152,6 +1207,7 @@ rak_status rak_batch_capture(rak_ctx *ctx, rak_batch *b, const uint32_t *q, cons
   if (!ctx || !b || !membership) return RAK_ERR_INVALID_ARGUMENT;
   Resolved r;
   RAK_CHECK(resolve(ctx, o, &r));
+  RAK_CHECK(ids_only(ctx, o, &r));
   RAK_TRY(ctx, cudaSetDevice(ctx->device));
   RAK_CHECK(batch_prepare(ctx, b, r));  // allocations happen before the capture
   if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
@@ -1588,6 +1644,7 @@ rak_status rak_server_create(rak_ctx *ctx, const rak_server_options *o, rak_serv
   s->device = ctx->device;
   s->opt = *o;
   rak_status st = resolve(ctx, &o->run, &s->run);
+  if (st == RAK_OK) st = ids_only(ctx, &o->run, &s->run);
   if (st != RAK_OK) { delete s; return st; }
   s->grid_cap = std::max(1, ctx->sms * 3 / o->slots);
   for (int i = 0; i < o->slots; ++i) {

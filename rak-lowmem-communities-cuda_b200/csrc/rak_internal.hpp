@@ -129,6 +129,13 @@ cudaError_t plan_sort(uint32_t *keys_in, uint32_t *keys_out, uint32_t *vals_in, 
                       int64_t n, int end_bit, void *temp, size_t *temp_bytes, cudaStream_t st);
 cudaError_t launch_init(uint32_t *vcom0, uint32_t *vcom1, const uint32_t *q, int64_t n, cudaStream_t st);
 cudaError_t launch_init_flags(uint8_t *aff0, uint8_t *aff1, const uint8_t *f, int64_t n, cudaStream_t st);
+// The reference GPU path's vertex order (partition by degree < 4, then < 128): ks (order) and pos
+// (its inverse), and the label mappings between positions in it and vertex ids.
+size_t ref_order_scratch_bytes(int64_t n);
+cudaError_t ref_order(const void *off, bool off64, int64_t n, uint32_t *ks, uint32_t *pos, void *scratch,
+                      cudaStream_t st);
+cudaError_t launch_init_mapped(uint32_t *vcom0, const uint32_t *q, const uint32_t *pos, int64_t n, cudaStream_t st);
+cudaError_t launch_labels_to_ids(uint32_t *m, const uint32_t *ks, int64_t n, cudaStream_t st);
 cudaError_t launch_hub_degrees(const void *off, bool off64, const uint32_t *order, int64_t nhub,
                                int64_t *deg, cudaStream_t st);
 cudaError_t launch_modularity(const void *off, bool off64, const uint32_t *tgt, const float *wt,

@@ -1,5 +1,6 @@
 // rak_kernels.cu -- plan building, validation, initialisation and FP64 modularity kernels.
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include "rak_device.cuh"
 #include "rak_internal.hpp"
@@ -66,6 +67,60 @@ __global__ void k_init_labels(uint32_t *v0, uint32_t *v1, const uint32_t *q, int
     v0[u] = c;
     if (v1) v1[u] = c;
   }
+}
+
+// Labels as positions in the reference's vertex order: v[u] = pos[q ? q[u] : u].
+__global__ void k_init_labels_mapped(uint32_t *v0, const uint32_t *q, const uint32_t *pos, int64_t n) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t u = tid; u < n; u += nt) v0[u] = __ldg(pos + (q ? q[u] : uint32_t(u)));
+}
+
+// Positions back to vertex ids: m[u] = ks[m[u]].
+__global__ void k_labels_to_ids(uint32_t *m, const uint32_t *ks, int64_t n) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t u = tid; u < n; u += nt) m[u] = __ldg(ks + m[u]);
+}
+
+// One pass of a two-pointer partition over a[lo..n): f[i - lo] = deg(a[i]) < limit.
+template <class O>
+__global__ void k_part_flags(const O *off, const uint32_t *a, int64_t lo, int64_t n, int64_t limit, uint32_t *f) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = lo + tid; i < n; i += nt) {
+    const uint32_t v = a[i];
+    f[i - lo] = int64_t(off[v + 1]) - int64_t(off[v]) < limit ? 1u : 0u;
+  }
+}
+
+// With pp the exclusive prefix count of f over the pass range and cnt matching elements: the k-th
+// non-matching element left of cnt (a hole, ranked from the left) and the k-th matching element
+// from cnt on (a mover, ranked from the right) form the k-th swapped pair.
+__global__ void k_part_ranks(const uint32_t *f, const uint32_t *pp, int64_t len, int64_t cnt, uint32_t *holepos,
+                             uint32_t *moverpos) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = tid; i < len; i += nt) {
+    if (i < cnt && !f[i]) holepos[i - pp[i]] = uint32_t(i);
+    if (i >= cnt && f[i]) moverpos[cnt - pp[i] - 1] = uint32_t(i);
+  }
+}
+
+__global__ void k_part_swap(uint32_t *a, int64_t lo, const uint32_t *holepos, const uint32_t *moverpos, int64_t pairs) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t k = tid; k < pairs; k += nt) {
+    const int64_t h = lo + holepos[k], m = lo + moverpos[k];
+    const uint32_t t = a[h];
+    a[h] = a[m];
+    a[m] = t;
+  }
+}
+
+__global__ void k_iota(uint32_t *a, int64_t n) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = tid; i < n; i += nt) a[i] = uint32_t(i);
+}
+
+__global__ void k_inverse(const uint32_t *ks, uint32_t *pos, int64_t n) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = tid; i < n; i += nt) pos[ks[i]] = uint32_t(i);
 }
 
 __global__ void k_init_flags(uint8_t *f0, uint8_t *f1, const uint8_t *f, int64_t n) {
@@ -341,6 +396,64 @@ cudaError_t launch_hub_degrees(const void *off, bool off64, const uint32_t *orde
 
 cudaError_t launch_init(uint32_t *vcom0, uint32_t *vcom1, const uint32_t *q, int64_t n, cudaStream_t st) {
   k_init_labels<<<grid_for(n, 4), TPB, 0, st>>>(vcom0, vcom1, q, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_init_mapped(uint32_t *vcom0, const uint32_t *q, const uint32_t *pos, int64_t n, cudaStream_t st) {
+  k_init_labels_mapped<<<grid_for(n, 4), TPB, 0, st>>>(vcom0, q, pos, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_labels_to_ids(uint32_t *m, const uint32_t *ks, int64_t n, cudaStream_t st) {
+  k_labels_to_ids<<<grid_for(n, 4), TPB, 0, st>>>(m, ks, n);
+  return cudaGetLastError();
+}
+
+size_t ref_order_scratch_bytes(int64_t n) {
+  size_t scan = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, scan, static_cast<const uint32_t *>(nullptr), static_cast<uint32_t *>(nullptr),
+                                n > 0 ? n : 1);
+  return size_t(n > 0 ? n : 1) * 16 + ((scan + 255) / 256) * 256 + 256;
+}
+
+// The vertex order of the reference's GPU path (inc/rakLowmemCuda.hxx:505-519, 563): vertex ids in
+// order, partitioned by degree < 4, then the rest by degree < 128, each with the two-pointer
+// exchange of libstdc++'s std::partition -- restated with parallel prefix counts. ks[i] is the
+// i-th vertex of that order, pos its inverse.
+cudaError_t ref_order(const void *off, bool off64, int64_t n, uint32_t *ks, uint32_t *pos, void *scratch,
+                      cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  uint32_t *f = static_cast<uint32_t *>(scratch), *pp = f + n, *hole = pp + n, *mover = hole + n;
+  void *cub_temp = mover + n;
+  size_t cub_bytes = ref_order_scratch_bytes(n) - size_t(n) * 16 - 256;
+  k_iota<<<grid_for(n, 4), TPB, 0, st>>>(ks, n);
+  int64_t lo = 0;
+  for (int pass = 0; pass < 2; ++pass) {
+    const int64_t len = n - lo, limit = pass == 0 ? 4 : 128;
+    if (len <= 0) break;
+    if (off64) k_part_flags<int64_t><<<grid_for(len, 4), TPB, 0, st>>>(static_cast<const int64_t *>(off), ks, lo, n, limit, f);
+    else k_part_flags<int32_t><<<grid_for(len, 4), TPB, 0, st>>>(static_cast<const int32_t *>(off), ks, lo, n, limit, f);
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(cub_temp, cub_bytes, f, pp, len, st);
+    if (e != cudaSuccess) return e;
+    uint32_t tail[2] = {0, 0};
+    if ((e = cudaMemcpyAsync(&tail[0], pp + len - 1, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(&tail[1], f + len - 1, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    const int64_t cnt = int64_t(tail[0]) + int64_t(tail[1]);
+    k_part_ranks<<<grid_for(len, 4), TPB, 0, st>>>(f, pp, len, cnt, hole, mover);
+    // pairs = non-matching elements left of cnt (= matching ones from cnt on) = cnt - pp[cnt]
+    int64_t pairs = 0;
+    if (cnt > 0 && cnt < len) {
+      uint32_t ppc = 0;
+      if ((e = cudaMemcpyAsync(&ppc, pp + cnt, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+      if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+      pairs = cnt - int64_t(ppc);
+    }
+    if (pairs > 0) k_part_swap<<<grid_for(pairs, 4), TPB, 0, st>>>(ks, lo, hole, mover, pairs);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    lo += cnt;
+  }
+  k_inverse<<<grid_for(n, 4), TPB, 0, st>>>(ks, pos, n);
   return cudaGetLastError();
 }
 

@@ -462,15 +462,15 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
   }
 }
 
-// The rule set of a work item: the asynchronous mode follows the reference GPU rules, the exact
-// synchronous mode the CPU rules, and the synchronous split mode either, per launch (a.gpu_rule).
+// The rule set of a work item: the exact synchronous mode follows the CPU rules; the split-layout
+// modes (asynchronous and synchronous split) either, per launch (a.gpu_rule).
 #define RAK_BY_RULE(F, ARGS)                                                            \
   do {                                                                                 \
-    if constexpr (MODE == MODE_SPLIT) {                                                \
+    if constexpr (MODE != MODE_SYNC) {                                                 \
       if (a.gpu_rule) F<S, MODE, O, UNIT, BATCH, RULE_GPU> ARGS;                       \
       else F<S, MODE, O, UNIT, BATCH, RULE_CPU> ARGS;                                  \
     } else {                                                                           \
-      F<S, MODE, O, UNIT, BATCH, MODE == MODE_ASYNC ? RULE_GPU : RULE_CPU> ARGS;       \
+      F<S, MODE, O, UNIT, BATCH, RULE_CPU> ARGS;                                       \
     }                                                                                  \
   } while (0)
 

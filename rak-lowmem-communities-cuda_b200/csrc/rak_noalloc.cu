@@ -116,6 +116,9 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   const bool exact = mode == RAK_MODE_SYNC, sync = mode != RAK_MODE_ASYNC;
   const int rescan = o->rescan < 0 ? (exact ? 1 : 0) : (o->rescan ? 1 : 0);
   if (rescan && !exact && slots > 1) return RAK_ERR_UNSUPPORTED;
+  if (o->sketch_rule > 2 || o->label_order > 2) return RAK_ERR_INVALID_ARGUMENT;
+  // the reference label order needs its own n-sized tables: this entry labels by vertex id
+  if ((exact && o->sketch_rule == 2) || o->label_order == 2) return RAK_ERR_UNSUPPORTED;
   const int iters = o->max_iterations;
   if (iters < 0 || iters > 1024 || !(o->tolerance >= 0)) return RAK_ERR_INVALID_ARGUMENT;
   Layout ly;
@@ -246,7 +249,8 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   a.pickless_step = o->pickless_step < 0 ? (mode == RAK_MODE_ASYNC ? 8 : 0) : o->pickless_step;
   a.check_on_pickless = o->check_on_pickless < 0 ? (mode == RAK_MODE_ASYNC ? 0 : 1) : (o->check_on_pickless ? 1 : 0);
   a.rescan = rescan;
-  a.gpu_rule = mode == RAK_MODE_SYNC_SPLIT && o->sketch_rule == 2;  // ASYNC: GPU rules, SYNC: CPU rules, fixed
+  // rule sets as in rak_lowmem_cuda: the CPU rules unless sketch_rule asks for the GPU ones
+  a.gpu_rule = mode != RAK_MODE_SYNC && o->sketch_rule == 2;
   a.timeout_ns = 20LL * 1000 * 1000 * 1000;
   if (iters > 0) {
     int grid = 0;

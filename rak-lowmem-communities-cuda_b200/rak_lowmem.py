@@ -43,7 +43,7 @@ class rak_options(C.Structure):
                 ("pickless_step", C.c_int32), ("check_on_pickless", C.c_int32), ("lane_max", C.c_int32),
                 ("hub_min", C.c_int32), ("hub_chunk", C.c_int32), ("validate", C.c_int32),
                 ("compute_modularity", C.c_int32), ("start_iteration", C.c_int32),
-                ("initial_flags", C.c_void_p), ("sketch_rule", C.c_int32), ("reserved32", C.c_int32),
+                ("initial_flags", C.c_void_p), ("sketch_rule", C.c_int32), ("label_order", C.c_int32),
                 ("reserved", C.c_int64 * 7)]
 
 
@@ -147,6 +147,7 @@ _sig("rak_host_csr_free", None, C.POINTER(rak_host_csr))
 _sig("rak_gen_rmat_device", C.c_int, P, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64,
      C.c_float, C.c_float, C.c_int32, C.POINTER(rak_csr))
 _sig("rak_device_csr_free", C.c_int, C.POINTER(rak_csr))
+_sig("rak_reference_vertex_order", C.c_int, P, C.POINTER(rak_csr), P)
 _sig("rak_read_mtx", C.c_int, C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(rak_host_csr))
 _sig("rak_device_csr_to_host", C.c_int, C.POINTER(rak_csr), C.POINTER(rak_host_csr))
 _sig("rak_csr_validate_host", C.c_int, C.POINTER(rak_csr))
@@ -427,6 +428,10 @@ class Context:
             qp = q.ctypes.data
         _check(_lib.rak_lowmem_cuda(self._c, C.byref(c), qp, C.byref(o), out.ctypes.data, C.byref(r)), self._c)
         return out, Result.of(r)
+
+    def reference_vertex_order(self, csr: rak_csr, ks):
+        """rak_reference_vertex_order into the torch CUDA tensor ks (n entries)."""
+        _check(_lib.rak_reference_vertex_order(self._c, C.byref(csr), ks.data_ptr()), self._c)
 
     def lowmem_device(self, csr: rak_csr, membership, q=None, **opts):
         """The same on a device-located csr; membership (and q) are torch CUDA tensors."""

@@ -109,3 +109,19 @@ def test_batch_rejects_bad_local_ids(ctx):
     with pytest.raises(rl.RakError) as e:
         rl.Batch(ctx, bad)
     assert e.value.status == 2
+
+
+def test_batch_refuses_reference_label_order(ctx):
+    """Batched graphs are labelled by local id; an explicit request for the reference label order
+    is refused rather than ignored."""
+    import torch
+    hb = rl.HostBatch.concat(mixed_graphs(False)[:3])
+    b = rl.Batch(ctx, hb)
+    out = torch.empty(hb.n, dtype=torch.int32, device="cuda")
+    with pytest.raises(rl.RakError) as e:
+        b.launch(out, label_order=2)
+    assert e.value.status == 7
+    b.launch(out, label_order=1)
+    it, _ = b.results()
+    assert (it >= 1).all()
+    b.close()

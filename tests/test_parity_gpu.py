@@ -262,10 +262,13 @@ def test_sync_split_gpu_rule_matches_oracle(ctx, name, slots, layout):
 
 def test_sketch_rule_mode_combinations(ctx):
     g = GRAPHS["rmat10"]
-    for mode, rule in ((rl.MODE_ASYNC, 1), (rl.MODE_SYNC, 2)):
-        with pytest.raises(rl.RakError) as e:
-            ctx.lowmem(g, mode=mode, sketch_rule=rule)
-        assert e.value.status == 7
+    with pytest.raises(rl.RakError) as e:
+        ctx.lowmem(g, mode=rl.MODE_SYNC, sketch_rule=2)
+    assert e.value.status == 7
     with pytest.raises(rl.RakError) as e:
         ctx.lowmem(g, sketch_rule=3)
     assert e.value.status == 1
+    for rule in (1, 2):                                # the asynchronous mode runs either rule set
+        lab, res = ctx.lowmem(g, sketch_rule=rule, compute_modularity=1)
+        assert lab.max() < g.n and res.iterations >= 1
+        assert res.modularity == pytest.approx(orc.modularity(orc.Graph.of(g), lab), rel=1e-9, abs=1e-12)

@@ -68,3 +68,16 @@ def test_noalloc_refuses_graphs_beyond_the_array():
         rl.lowmem_noalloc(0, None, csr, out)
     assert e.value.status == 3
     assert "bytes of scratch" in str(e.value)
+
+
+def test_noalloc_labels_by_id_only():
+    import torch
+    g = rl.gen_rmat(10, 8, seed=25)
+    keep, csr = device_graph(g)
+    out = torch.empty(g.n, dtype=torch.int32, device="cuda")
+    with pytest.raises(rl.RakError) as e:
+        rl.lowmem_noalloc(0, None, csr, out, label_order=2)
+    assert e.value.status == 7
+    res = rl.lowmem_noalloc(0, None, csr, out, label_order=1, sketch_rule=2)
+    torch.cuda.synchronize()
+    assert res.iterations >= 1 and int(out.max()) < g.n
