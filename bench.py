@@ -325,13 +325,13 @@ def batched_leg(ctx, count, steps, threads, stream):
     for i, (_, rg) in enumerate(members):   # warm-up: one run of every member
         a, z = int(hb.graph_offsets[i]), int(hb.graph_offsets[i + 1])
         if z > a:
-            rg.run(loop_lab[a:z])
+            rg.run(loop_lab[a:z], label_order=1)
     e0.record(stream)
     for _ in range(steps):
         for i, (_, rg) in enumerate(members):
             a, z = int(hb.graph_offsets[i]), int(hb.graph_offsets[i + 1])
             if z > a:
-                rg.run(loop_lab[a:z])
+                rg.run(loop_lab[a:z], label_order=1)
     e1.record(stream)
     torch.cuda.synchronize()
     t_loop = e0.elapsed_time(e1) / 1e3 / steps
@@ -352,7 +352,8 @@ def batched_leg(ctx, count, steps, threads, stream):
             "graphs_per_s": count / t_batch, "ms_per_batch": 1e3 * t_batch,
             "loop_graphs_per_s": count / t_loop, "loop_ms": 1e3 * t_loop, "speedup": t_loop / t_batch,
             "batched_path": "rak_batch_capture + rak_batch_replay (one persistent launch in a CUDA graph)",
-            "loop_path": "rak_graph_run per resident graph (one persistent launch + read-back each)",
+            "loop_path": "rak_graph_run per resident graph (one persistent launch + read-back each), labels by "
+                         "vertex id as in the batch (label_order 1)",
             "edges_per_s": tot.traversed_edges / t_batch, "iterations_max": int(iters.max()),
             "modularity_mean": float(np.mean(q_batch)), "loop_modularity_mean": float(np.mean(q_loop)),
             "nmi_sbm_mean": float(np.mean(nmis)) if nmis else None,
@@ -376,8 +377,10 @@ def serving_leg(ctx, rates, seconds, threads, seed=11):
     graphs = pool + [big]
     log(f"[serving] pool of {len(pool)} + scale-22 R-MAT ({big.m} edges) generated in {time.time() - t0:.1f}s")
     assert all(rl.validate_host(g) == 0 for g in graphs)
-    q_alone = [ctx.modularity(g, ctx.lowmem(g)[0]) for g in graphs]
-    q_again = [ctx.modularity(g, ctx.lowmem(g)[0]) for g in graphs]   # control: alone, run again
+    # alone with the served path's labelling (vertex ids): the same algorithm, so the ratio isolates
+    # the effect of batching and overlap
+    q_alone = [ctx.modularity(g, ctx.lowmem(g, label_order=1)[0]) for g in graphs]
+    q_again = [ctx.modularity(g, ctx.lowmem(g, label_order=1)[0]) for g in graphs]   # control: alone, run again
 
     def quality(q_of):
         """Served (or repeated) modularity against the first run alone: the edge-weighted ratio,
@@ -648,6 +651,8 @@ def main():
         last = results[-1]
         cfg = describe(args.workload, spec, g)
         cfg.update(slots=args.slots, mode="async (in-place, pickless every 8th iteration)",
+                   rules="reference CPU sketch rules (last free slot, clamped decrement, linear argmax)",
+                   labels="start at positions of the reference degree-partition order; returned as vertex ids",
                    parallelism=f"replicas x{world}" if world > 1 else "single GPU",
                    l2=f"inputs larger than L2: graph {graph_bytes(g, spec['off_bits']) / 1e9:.1f} GB vs 126 MB L2")
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
