@@ -353,7 +353,7 @@ def batched_leg(ctx, count, steps, threads, stream):
             "loop_graphs_per_s": count / t_loop, "loop_ms": 1e3 * t_loop, "speedup": t_loop / t_batch,
             "batched_path": "rak_batch_capture + rak_batch_replay (one persistent launch in a CUDA graph)",
             "loop_path": "rak_graph_run per resident graph (one persistent launch + read-back each), labels by "
-                         "vertex id as in the batch (label_order 1)",
+                         "vertex id as the batch's default (label_order 1)",
             "edges_per_s": tot.traversed_edges / t_batch, "iterations_max": int(iters.max()),
             "modularity_mean": float(np.mean(q_batch)), "loop_modularity_mean": float(np.mean(q_loop)),
             "nmi_sbm_mean": float(np.mean(nmis)) if nmis else None,
@@ -377,8 +377,8 @@ def serving_leg(ctx, rates, seconds, threads, seed=11):
     graphs = pool + [big]
     log(f"[serving] pool of {len(pool)} + scale-22 R-MAT ({big.m} edges) generated in {time.time() - t0:.1f}s")
     assert all(rl.validate_host(g) == 0 for g in graphs)
-    # alone with the served path's labelling (vertex ids): the same algorithm, so the ratio isolates
-    # the effect of batching and overlap
+    # alone with the served path's default labelling (vertex ids): the same algorithm, so the
+    # ratio isolates the effect of batching and overlap
     q_alone = [ctx.modularity(g, ctx.lowmem(g, label_order=1)[0]) for g in graphs]
     q_again = [ctx.modularity(g, ctx.lowmem(g, label_order=1)[0]) for g in graphs]   # control: alone, run again
 

@@ -100,9 +100,10 @@ typedef struct rak_options {
   int32_t label_order;        /* -1 or 0: mode default; 1: labels are vertex ids; 2: labels are
                                  positions in the reference GPU path's vertex order (degree
                                  partition, inc/rakLowmemCuda.hxx:505-519, 563), which its pickless
-                                 rule compares; results are vertex ids either way. ASYNC: 2 [2];
-                                 SYNC modes: 1 only. Graph steps, batches, the server and the
-                                 no-alloc entry label by id and refuse 2 */
+                                 rule compares; results are vertex ids either way; in a batch,
+                                 each graph's own order. Single-graph ASYNC runs: 2 [2]; batches
+                                 and the server: 1 [1], 2 on request; SYNC modes: 1 only. Graph
+                                 steps and the no-alloc entry label by id and refuse 2 */
   int64_t reserved[7];
 } rak_options;
 
@@ -361,6 +362,9 @@ rak_status rak_device_csr_free(rak_csr *g);
  * exchange), whose positions name the labels of asynchronous runs (rak_options.label_order).
  * g device-located; ks: device, n entries (ks[i] = i-th vertex). */
 rak_status rak_reference_vertex_order(rak_ctx *ctx, const rak_csr *g, uint32_t *ks);
+/* The same order for every graph of a batch: ks (device, the batch's n entries) holds, in each
+ * graph's range, that graph's local vertex ids in its reference order. */
+rak_status rak_batch_reference_vertex_order(rak_ctx *ctx, rak_batch *b, uint32_t *ks);
 /* Copies a device-located CSR into newly allocated host arrays (offsets widened to 64 bits); free
  * them with rak_host_csr_free. */
 rak_status rak_device_csr_to_host(const rak_csr *g, rak_host_csr *out);

@@ -131,9 +131,10 @@ cudaError_t launch_init(uint32_t *vcom0, uint32_t *vcom1, const uint32_t *q, int
 cudaError_t launch_init_flags(uint8_t *aff0, uint8_t *aff1, const uint8_t *f, int64_t n, cudaStream_t st);
 // The reference GPU path's vertex order (partition by degree < 4, then < 128): ks (order) and pos
 // (its inverse), and the label mappings between positions in it and vertex ids.
-size_t ref_order_scratch_bytes(int64_t n);
-cudaError_t ref_order(const void *off, bool off64, int64_t n, uint32_t *ks, uint32_t *pos, void *scratch,
-                      cudaStream_t st);
+// gid/vbase/ngraphs: the graphs of a batch (ks, pos in global vertex indices), or null/0 for one graph.
+size_t ref_order_scratch_bytes(int64_t n, int64_t ngraphs);
+cudaError_t ref_order(const void *off, bool off64, int64_t n, const uint32_t *gid, const int64_t *vbase,
+                      int64_t ngraphs, uint32_t *ks, uint32_t *pos, void *scratch, cudaStream_t st);
 cudaError_t launch_init_mapped(uint32_t *vcom0, const uint32_t *q, const uint32_t *pos, int64_t n, cudaStream_t st);
 cudaError_t launch_labels_to_ids(uint32_t *m, const uint32_t *ks, int64_t n, cudaStream_t st);
 cudaError_t launch_hub_degrees(const void *off, bool off64, const uint32_t *order, int64_t nhub,
@@ -170,6 +171,11 @@ cudaError_t launch_batch_validate(const int64_t *vbase, int64_t ngraphs, int64_t
                                   const uint32_t *tgt, const uint32_t *gid, unsigned int *bad, cudaStream_t st);
 cudaError_t launch_batch_init(uint32_t *v0, uint32_t *v1, const uint32_t *q, const uint32_t *gid,
                               const int64_t *vbase, int64_t n, cudaStream_t st);
+// Batch labels as global positions in each graph's reference order (q local), and back to local ids.
+cudaError_t launch_batch_init_mapped(uint32_t *v0, const uint32_t *q, const uint32_t *gid, const int64_t *vbase,
+                                     const uint32_t *pos, int64_t n, cudaStream_t st);
+cudaError_t launch_batch_finish_mapped(const uint32_t *v0, const uint32_t *ks, const uint32_t *gid,
+                                       const int64_t *vbase, int64_t n, uint32_t *membership, cudaStream_t st);
 cudaError_t launch_batch_finish(const uint32_t *v0, const uint32_t *v1, const void *rs, const uint32_t *gid,
                                 const int64_t *vbase, int64_t n, uint32_t *membership, cudaStream_t st);
 cudaError_t launch_batch_modularity(const int64_t *off, const uint32_t *tgt, const float *wt, const uint32_t *gid,

@@ -81,35 +81,70 @@ __global__ void k_labels_to_ids(uint32_t *m, const uint32_t *ks, int64_t n) {
   for (int64_t u = tid; u < n; u += nt) m[u] = __ldg(ks + m[u]);
 }
 
-// One pass of a two-pointer partition over a[lo..n): f[i - lo] = deg(a[i]) < limit.
+// The reference GPU path's vertex order, per segment (one graph of a batch, or the whole graph):
+// vertex ids in order, partitioned by degree < 4, then the rest by degree < 128, each pass with the
+// two-pointer exchange of libstdc++'s std::partition. For a pass over the range [lo, e) of a
+// segment with c matching elements: the k-th non-matching element left of lo + c (a hole, ranked
+// from the left) swaps with the k-th matching element from lo + c on (a mover, ranked from the
+// right). Ranks come from one exclusive prefix count P of the match flags over all segments; flags
+// are 0 left of lo, so P[i] - P[b] counts the matches in [lo, i).
+struct Seg {
+  int64_t b, e;
+  uint32_t g;
+};
+__device__ __forceinline__ Seg seg_of(const uint32_t *gid, const int64_t *vbase, int64_t n, int64_t i) {
+  if (!gid) return {0, n, 0u};
+  const uint32_t g = gid[i];
+  return {vbase[g], vbase[g + 1], g};
+}
+
 template <class O>
-__global__ void k_part_flags(const O *off, const uint32_t *a, int64_t lo, int64_t n, int64_t limit, uint32_t *f) {
+__global__ void k_ro_flags(const O *off, const uint32_t *ks, int64_t n, const uint32_t *gid, const int64_t *vbase,
+                           const uint32_t *lo_cnt, int64_t limit, uint32_t *f) {
   const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
-  for (int64_t i = lo + tid; i < n; i += nt) {
-    const uint32_t v = a[i];
-    f[i - lo] = int64_t(off[v + 1]) - int64_t(off[v]) < limit ? 1u : 0u;
+  for (int64_t i = tid; i <= n; i += nt) {
+    if (i == n) { f[n] = 0u; continue; }
+    const Seg s = seg_of(gid, vbase, n, i);
+    const int64_t lo = s.b + (lo_cnt ? lo_cnt[s.g] : 0u);
+    const uint32_t v = ks[i];
+    f[i] = i >= lo && int64_t(off[v + 1]) - int64_t(off[v]) < limit ? 1u : 0u;
   }
 }
 
-// With pp the exclusive prefix count of f over the pass range and cnt matching elements: the k-th
-// non-matching element left of cnt (a hole, ranked from the left) and the k-th matching element
-// from cnt on (a mover, ranked from the right) form the k-th swapped pair.
-__global__ void k_part_ranks(const uint32_t *f, const uint32_t *pp, int64_t len, int64_t cnt, uint32_t *holepos,
-                             uint32_t *moverpos) {
+// Matches per segment: cnt[g] = P[e] - P[b].
+__global__ void k_ro_count(const uint32_t *P, const int64_t *vbase, int64_t ngraphs, int64_t n, uint32_t *cnt) {
   const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
-  for (int64_t i = tid; i < len; i += nt) {
-    if (i < cnt && !f[i]) holepos[i - pp[i]] = uint32_t(i);
-    if (i >= cnt && f[i]) moverpos[cnt - pp[i] - 1] = uint32_t(i);
+  for (int64_t g = tid; g < ngraphs; g += nt) {
+    const int64_t b = vbase ? vbase[g] : 0, e = vbase ? vbase[g + 1] : n;
+    cnt[g] = P[e] - P[b];
   }
 }
 
-__global__ void k_part_swap(uint32_t *a, int64_t lo, const uint32_t *holepos, const uint32_t *moverpos, int64_t pairs) {
+__global__ void k_ro_movers(const uint32_t *f, const uint32_t *P, int64_t n, const uint32_t *gid, const int64_t *vbase,
+                            const uint32_t *lo_cnt, const uint32_t *cnt, uint32_t *mover) {
   const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
-  for (int64_t k = tid; k < pairs; k += nt) {
-    const int64_t h = lo + holepos[k], m = lo + moverpos[k];
-    const uint32_t t = a[h];
-    a[h] = a[m];
-    a[m] = t;
+  for (int64_t i = tid; i < n; i += nt) {
+    if (!f[i]) continue;
+    const Seg s = seg_of(gid, vbase, n, i);
+    const int64_t lo = s.b + (lo_cnt ? lo_cnt[s.g] : 0u), c = cnt[s.g];
+    const int64_t pp = int64_t(P[i]) - int64_t(P[s.b]);
+    if (i - lo >= c) mover[lo + (c - pp - 1)] = uint32_t(i - s.b);
+  }
+}
+
+__global__ void k_ro_swap(const uint32_t *f, const uint32_t *P, int64_t n, const uint32_t *gid, const int64_t *vbase,
+                          const uint32_t *lo_cnt, const uint32_t *cnt, const uint32_t *mover, uint32_t *ks) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = tid; i < n; i += nt) {
+    if (f[i]) continue;
+    const Seg s = seg_of(gid, vbase, n, i);
+    const int64_t lo = s.b + (lo_cnt ? lo_cnt[s.g] : 0u), c = cnt[s.g];
+    if (i < lo || i - lo >= c) continue;
+    const int64_t pp = int64_t(P[i]) - int64_t(P[s.b]);
+    const int64_t j = s.b + mover[lo + (i - lo - pp)];
+    const uint32_t t = ks[i];
+    ks[i] = ks[j];
+    ks[j] = t;
   }
 }
 
@@ -225,6 +260,21 @@ __global__ void k_batch_init(uint32_t *v0, uint32_t *v1, const uint32_t *q, cons
     v0[u] = c;
     if (v1) v1[u] = c;
   }
+}
+
+// Labels of an asynchronous batch run in the reference order: global position of the (local)
+// initial label within its graph's order.
+__global__ void k_batch_init_mapped(uint32_t *v0, const uint32_t *q, const uint32_t *gid, const int64_t *vbase,
+                                    const uint32_t *pos, int64_t n) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t u = tid; u < n; u += nt) v0[u] = __ldg(pos + (q ? uint32_t(vbase[gid[u]]) + q[u] : uint32_t(u)));
+}
+
+// Global positions back to local vertex ids.
+__global__ void k_batch_finish_mapped(const uint32_t *v0, const uint32_t *ks, const uint32_t *gid,
+                                      const int64_t *vbase, int64_t n, uint32_t *membership) {
+  const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t u = tid; u < n; u += nt) membership[u] = __ldg(ks + v0[u]) - uint32_t(vbase[gid[u]]);
 }
 
 // Final local labels: the buffer the last iteration wrote (decided on the device from the
@@ -345,6 +395,18 @@ cudaError_t launch_batch_init(uint32_t *v0, uint32_t *v1, const uint32_t *q, con
   return cudaGetLastError();
 }
 
+cudaError_t launch_batch_init_mapped(uint32_t *v0, const uint32_t *q, const uint32_t *gid, const int64_t *vbase,
+                                     const uint32_t *pos, int64_t n, cudaStream_t st) {
+  k_batch_init_mapped<<<grid_for(n, 4), TPB, 0, st>>>(v0, q, gid, vbase, pos, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_finish_mapped(const uint32_t *v0, const uint32_t *ks, const uint32_t *gid,
+                                       const int64_t *vbase, int64_t n, uint32_t *membership, cudaStream_t st) {
+  k_batch_finish_mapped<<<grid_for(n, 4), TPB, 0, st>>>(v0, ks, gid, vbase, n, membership);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_batch_finish(const uint32_t *v0, const uint32_t *v1, const void *rs, const uint32_t *gid,
                                 const int64_t *vbase, int64_t n, uint32_t *membership, cudaStream_t st) {
   k_batch_finish<<<grid_for(n, 4), TPB, 0, st>>>(v0, v1, static_cast<const RunState *>(rs), gid, vbase, n, membership);
@@ -409,49 +471,40 @@ cudaError_t launch_labels_to_ids(uint32_t *m, const uint32_t *ks, int64_t n, cud
   return cudaGetLastError();
 }
 
-size_t ref_order_scratch_bytes(int64_t n) {
+size_t ref_order_scratch_bytes(int64_t n, int64_t ngraphs) {
   size_t scan = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, scan, static_cast<const uint32_t *>(nullptr), static_cast<uint32_t *>(nullptr),
-                                n > 0 ? n : 1);
-  return size_t(n > 0 ? n : 1) * 16 + ((scan + 255) / 256) * 256 + 256;
+                                n + 1);
+  const size_t arrays = size_t(n + 1) * 4 * 2 + size_t(n > 0 ? n : 1) * 4 + size_t(ngraphs > 0 ? ngraphs : 1) * 4 * 2;
+  return ((arrays + 255) / 256) * 256 + ((scan + 255) / 256) * 256 + 256;
 }
 
-// The vertex order of the reference's GPU path (inc/rakLowmemCuda.hxx:505-519, 563): vertex ids in
-// order, partitioned by degree < 4, then the rest by degree < 128, each with the two-pointer
-// exchange of libstdc++'s std::partition -- restated with parallel prefix counts. ks[i] is the
-// i-th vertex of that order, pos its inverse.
-cudaError_t ref_order(const void *off, bool off64, int64_t n, uint32_t *ks, uint32_t *pos, void *scratch,
-                      cudaStream_t st) {
+// The reference GPU path's vertex order (inc/rakLowmemCuda.hxx:505-519, 563) of every segment:
+// gid/vbase describe a batch (ngraphs graphs; ks and pos then hold global vertex indices), or are
+// null for one graph. ks[i] is the i-th vertex of that order, pos its inverse. No host round trip.
+cudaError_t ref_order(const void *off, bool off64, int64_t n, const uint32_t *gid, const int64_t *vbase,
+                      int64_t ngraphs, uint32_t *ks, uint32_t *pos, void *scratch, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  uint32_t *f = static_cast<uint32_t *>(scratch), *pp = f + n, *hole = pp + n, *mover = hole + n;
-  void *cub_temp = mover + n;
-  size_t cub_bytes = ref_order_scratch_bytes(n) - size_t(n) * 16 - 256;
+  if (!gid) ngraphs = 1;
+  uint8_t *p = static_cast<uint8_t *>(scratch);
+  uint32_t *f = reinterpret_cast<uint32_t *>(p), *P = f + (n + 1), *mover = P + (n + 1);
+  uint32_t *cnt1 = mover + n, *cnt2 = cnt1 + ngraphs;
+  const size_t arrays = size_t(n + 1) * 4 * 2 + size_t(n) * 4 + size_t(ngraphs) * 4 * 2;
+  void *cub_temp = p + ((arrays + 255) / 256) * 256;
+  size_t cub_bytes = ref_order_scratch_bytes(n, ngraphs) - ((arrays + 255) / 256) * 256 - 256;
   k_iota<<<grid_for(n, 4), TPB, 0, st>>>(ks, n);
-  int64_t lo = 0;
   for (int pass = 0; pass < 2; ++pass) {
-    const int64_t len = n - lo, limit = pass == 0 ? 4 : 128;
-    if (len <= 0) break;
-    if (off64) k_part_flags<int64_t><<<grid_for(len, 4), TPB, 0, st>>>(static_cast<const int64_t *>(off), ks, lo, n, limit, f);
-    else k_part_flags<int32_t><<<grid_for(len, 4), TPB, 0, st>>>(static_cast<const int32_t *>(off), ks, lo, n, limit, f);
-    cudaError_t e = cub::DeviceScan::ExclusiveSum(cub_temp, cub_bytes, f, pp, len, st);
+    const uint32_t *lo_cnt = pass == 0 ? nullptr : cnt1;
+    uint32_t *cnt = pass == 0 ? cnt1 : cnt2;
+    const int64_t limit = pass == 0 ? 4 : 128;
+    if (off64) k_ro_flags<int64_t><<<grid_for(n + 1, 4), TPB, 0, st>>>(static_cast<const int64_t *>(off), ks, n, gid, vbase, lo_cnt, limit, f);
+    else k_ro_flags<int32_t><<<grid_for(n + 1, 4), TPB, 0, st>>>(static_cast<const int32_t *>(off), ks, n, gid, vbase, lo_cnt, limit, f);
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(cub_temp, cub_bytes, f, P, n + 1, st);
     if (e != cudaSuccess) return e;
-    uint32_t tail[2] = {0, 0};
-    if ((e = cudaMemcpyAsync(&tail[0], pp + len - 1, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
-    if ((e = cudaMemcpyAsync(&tail[1], f + len - 1, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-    const int64_t cnt = int64_t(tail[0]) + int64_t(tail[1]);
-    k_part_ranks<<<grid_for(len, 4), TPB, 0, st>>>(f, pp, len, cnt, hole, mover);
-    // pairs = non-matching elements left of cnt (= matching ones from cnt on) = cnt - pp[cnt]
-    int64_t pairs = 0;
-    if (cnt > 0 && cnt < len) {
-      uint32_t ppc = 0;
-      if ((e = cudaMemcpyAsync(&ppc, pp + cnt, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
-      if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-      pairs = cnt - int64_t(ppc);
-    }
-    if (pairs > 0) k_part_swap<<<grid_for(pairs, 4), TPB, 0, st>>>(ks, lo, hole, mover, pairs);
+    k_ro_count<<<grid_for(ngraphs, 1), TPB, 0, st>>>(P, gid ? vbase : nullptr, ngraphs, n, cnt);
+    k_ro_movers<<<grid_for(n, 4), TPB, 0, st>>>(f, P, n, gid, vbase, lo_cnt, cnt, mover);
+    k_ro_swap<<<grid_for(n, 4), TPB, 0, st>>>(f, P, n, gid, vbase, lo_cnt, cnt, mover, ks);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    lo += cnt;
   }
   k_inverse<<<grid_for(n, 4), TPB, 0, st>>>(ks, pos, n);
   return cudaGetLastError();

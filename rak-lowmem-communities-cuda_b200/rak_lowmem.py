@@ -148,6 +148,7 @@ _sig("rak_gen_rmat_device", C.c_int, P, C.c_int, C.c_double, C.c_double, C.c_dou
      C.c_float, C.c_float, C.c_int32, C.POINTER(rak_csr))
 _sig("rak_device_csr_free", C.c_int, C.POINTER(rak_csr))
 _sig("rak_reference_vertex_order", C.c_int, P, C.POINTER(rak_csr), P)
+_sig("rak_batch_reference_vertex_order", C.c_int, P, P, P)
 _sig("rak_read_mtx", C.c_int, C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(rak_host_csr))
 _sig("rak_device_csr_to_host", C.c_int, C.POINTER(rak_csr), C.POINTER(rak_host_csr))
 _sig("rak_csr_validate_host", C.c_int, C.POINTER(rak_csr))
@@ -588,6 +589,11 @@ class Batch:
         _check(_lib.rak_batch_autotune(self.ctx.handle, self._b, self.graphs, C.byref(o), C.byref(sp),
                                        membership.data_ptr(), C.byref(best), log, 64, C.byref(n)), self.ctx.handle)
         return _tune_out(best, log, n.value)
+
+    def reference_vertex_order(self, ks):
+        """rak_batch_reference_vertex_order into the torch CUDA tensor ks (n entries): each graph's
+        local vertex ids in its reference order."""
+        _check(_lib.rak_batch_reference_vertex_order(self.ctx.handle, self._b, ks.data_ptr()), self.ctx.handle)
 
     def launch(self, membership, q=None, **opts):
         o = options(**opts)

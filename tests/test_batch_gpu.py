@@ -111,17 +111,28 @@ def test_batch_rejects_bad_local_ids(ctx):
     assert e.value.status == 2
 
 
-def test_batch_refuses_reference_label_order(ctx):
-    """Batched graphs are labelled by local id; an explicit request for the reference label order
-    is refused rather than ignored."""
+def test_batch_label_orders(ctx):
+    """Asynchronous batches run with either label order (ids by default, the reference order on
+    request) and captured launches replay with it; the synchronous modes label by id only."""
     import torch
-    hb = rl.HostBatch.concat(mixed_graphs(False)[:3])
+    gs = mixed_graphs(False)[:3]
+    hb = rl.HostBatch.concat(gs)
     b = rl.Batch(ctx, hb)
     out = torch.empty(hb.n, dtype=torch.int32, device="cuda")
+    for order in (1, 2):
+        b.launch(out, label_order=order)
+        it, _ = b.results()
+        lab = out.cpu().numpy().view(np.uint32)
+        for i, g in enumerate(gs):
+            a, z = int(hb.graph_offsets[i]), int(hb.graph_offsets[i + 1])
+            assert lab[a:z].max() < g.n and it[i] >= 1
+    b.capture(out, label_order=2)
+    for _ in range(2):
+        out.fill_(-1)
+        b.replay()
+        it, _ = b.results()
+        assert int(out.min()) >= 0 and (it >= 1).all()
     with pytest.raises(rl.RakError) as e:
-        b.launch(out, label_order=2)
+        b.launch(out, mode=rl.MODE_SYNC_SPLIT, label_order=2)
     assert e.value.status == 7
-    b.launch(out, label_order=1)
-    it, _ = b.results()
-    assert (it >= 1).all()
     b.close()

@@ -1,8 +1,9 @@
 """Label order of the asynchronous mode: labels are positions in the reference GPU path's vertex
 order (inc/rakLowmemCuda.hxx:505-519, 563) -- the order its pickless rule compares -- and come
 back as vertex ids. The device restatement of that order must equal the reference's own two
-std::partition calls (oracle bridge), and lattice-like graphs, whose ids follow the grid, must not
-stall under the pickless rule."""
+std::partition calls (oracle bridge), for one graph and for every graph of a batch (each graph
+partitioned on its own), and lattice-like graphs, whose ids follow the grid, must not stall under
+the pickless rule, alone or batched."""
 import numpy as np
 import pytest
 
@@ -66,3 +67,39 @@ def test_label_order_options(ctx):
     with pytest.raises(rl.RakError) as e:
         ctx.lowmem(g, mode=rl.MODE_SYNC, label_order=2)
     assert e.value.status == 7
+
+
+def test_batch_order_equals_reference_partition_per_graph(ctx):
+    import torch
+    gs = [CASES[k]() for k in sorted(CASES)] + [rl.gen_rmat(12, 16, seed=9), CASES["path"]()]
+    hb = rl.HostBatch.concat(gs)
+    b = rl.Batch(ctx, hb)
+    ks = torch.full((hb.n,), -1, dtype=torch.int32, device="cuda")
+    b.reference_vertex_order(ks)
+    got = ks.cpu().numpy().view(np.uint32)
+    for i, g in enumerate(gs):
+        a, z = int(hb.graph_offsets[i]), int(hb.graph_offsets[i + 1])
+        np.testing.assert_array_equal(got[a:z], orc.ref_vertex_order(g), err_msg=f"graph {i}")
+    b.close()
+
+
+@pytest.mark.parametrize("slots", [8, 1])
+def test_batched_lattice_does_not_stall(ctx, slots):
+    """With label_order 2 a batch runs each graph in its own reference order, like a single graph
+    (batches default to id labels)."""
+    import torch
+    gs = [rl.gen_lattice(256, 256, 0.05, 0.01, seed=11), rl.gen_rmat(12, 16, seed=12),
+          rl.gen_lattice(300, 200, 0.05, 0.01, seed=13)]
+    hb = rl.HostBatch.concat(gs)
+    b = rl.Batch(ctx, hb)
+    out = torch.empty(hb.n, dtype=torch.int32, device="cuda")
+    b.launch(out, slots=slots, label_order=2)
+    b.results()
+    q = b.modularity(out)
+    lab = out.cpu().numpy().view(np.uint32)
+    for i, g in enumerate(gs):
+        a, z = int(hb.graph_offsets[i]), int(hb.graph_offsets[i + 1])
+        assert lab[a:z].max() < g.n
+        assert q[i] == pytest.approx(orc.modularity(orc.Graph.of(g), lab[a:z]), rel=1e-9, abs=1e-12)
+    assert q[0] > 0.4 and q[2] > 0.4, q
+    b.close()
