@@ -336,19 +336,19 @@ rak_status validate_host_t(const O *off, const uint32_t *tgt, int64_t n, int64_t
 int nkeys_of(const Layout &ly) { return int(6 + ly.lane_max + 1); }
 
 // Region sizes, item counts and chunk table from the key histogram and split-vertex degrees.
-void regions_from(const std::vector<unsigned long long> &hist, const Layout &ly, int64_t nchunks, rak::Regions *rg) {
+void regions_from(const std::vector<unsigned long long> &hist, const Layout &ly, int64_t nchunks, int sms,
+                  rak::Regions *rg) {
   int64_t cnt[rak::NREG] = {};
   for (int k = 0; k < 6; ++k) cnt[k] = int64_t(hist[k]);
   for (int64_t k = 6; k < 6 + ly.lane_max; ++k) cnt[rak::REG_LANE] += int64_t(hist[k]);
+  rg->lane_item = rak::lane_item_for(cnt[rak::REG_LANE], int64_t(sms) * rak::LPA_WARPS_PER_SM);
   int64_t v = 0, it = 0;
   for (int r = 0; r < rak::NREG; ++r) {
     rg->vbegin[r] = v;
     rg->vcount[r] = cnt[r];
     v += cnt[r];
     rg->ibegin[r] = it;
-    const int G = rak::region_group(r);
-    if (r == rak::REG_HUB) it += nchunks;
-    else it += (cnt[r] * G + 31) / 32;
+    it += rak::region_items(r, cnt[r], nchunks, rg->lane_item);
   }
   rg->ibegin[rak::NREG] = it;
 }
@@ -410,7 +410,7 @@ rak_status build_plan(rak_ctx *ctx, rak_graph *gr, const Layout &ly, Tracker *tr
     RAK_TRY(ctx, cudaMemcpyAsync(gr->chunk_hub, ch.data(), ch.size() * 4, cudaMemcpyHostToDevice, st));
   }
   gr->plan_bytes = gr->p_order.bytes + gr->p_hub_first.bytes + gr->p_chunk_hub.bytes;
-  regions_from(h, ly, gr->nchunks, &gr->rg);
+  regions_from(h, ly, gr->nchunks, ctx->sms, &gr->rg);
   cudaEventRecord(ev.e[1], st);
   RAK_TRY(ctx, cudaStreamSynchronize(st));
   gr->plan_ms = ev.ms(0, 1);
@@ -517,7 +517,7 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
   a.sk_keys = b.skk.as<uint32_t>(); a.sk_wts = b.skw.as<float>();
   a.stats = b.stats.as<unsigned long long>(); a.rs = b.rs.p;
   a.iters = r.iters; a.start_iter = r.start; a.tolerance = r.tol; a.pickless_step = r.pickless;
-  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n); a.gpu_rule = r.rule == 2; a.timeout_ns = 20LL * 1000 * 1000 * 1000;
+  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = 20LL * 1000 * 1000 * 1000;
 
   // the kernel's module is loaded here, not inside the timed region
   if (r.iters > 0) RAK_TRY(ctx, rak::prepare_lpa(r.slots, r.mode, gr->off64, gr->wt == nullptr, false));
@@ -850,7 +850,7 @@ rak_status rak_graph_step(rak_ctx *ctx, rak_graph *gr, const rak_options *o, int
   a.sk_keys = b.skk.as<uint32_t>(); a.sk_wts = b.skw.as<float>();
   a.stats = b.stats.as<unsigned long long>(); a.rs = b.rs.p;
   a.iters = 1; a.start_iter = iteration; a.tolerance = r.tol; a.pickless_step = r.pickless;
-  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n); a.gpu_rule = r.rule == 2; a.timeout_ns = 20LL * 1000 * 1000 * 1000;
+  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = 20LL * 1000 * 1000 * 1000;
   int grid = 0;
   RAK_TRY(ctx, rak::launch_lpa(a, r.slots, r.mode, gr->off64, st, &grid));
   unsigned long long s[rak::STATS_STRIDE] = {};
@@ -1124,7 +1124,7 @@ rak_status batch_enqueue(rak_ctx *ctx, rak_batch *b, const uint32_t *q, const Re
     a.giters = b->giters.as<int32_t>(); a.gchanged = b->gchanged.as<unsigned long long>();
     a.running = b->running.as<unsigned int>(); a.ngraphs = G; a.grid_cap = grid_cap;
     a.iters = r.iters; a.start_iter = r.start; a.tolerance = r.tol; a.pickless_step = r.pickless;
-    a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n); a.gpu_rule = r.rule == 2; a.timeout_ns = 20LL * 1000 * 1000 * 1000;
+    a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = 20LL * 1000 * 1000 * 1000;
     int grid = 0;
     RAK_TRY(ctx, rak::launch_lpa(a, r.slots, r.mode, true, st, &grid, true));
   }

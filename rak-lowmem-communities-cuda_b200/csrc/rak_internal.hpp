@@ -19,10 +19,29 @@ constexpr int REG_HUB = 0;
 constexpr int REG_LANE = 6;
 __host__ __device__ constexpr int region_group(int r) { return r == REG_LANE ? 1 : (r == REG_HUB ? 32 : (64 >> r)); }
 
+// Work items of region r holding cnt vertices (nchunks: split-vertex chunks, region 0; lane_item:
+// batches of 32 one-lane vertices per item, region 6).
+__host__ __device__ inline int64_t region_items(int r, int64_t cnt, int64_t nchunks, int64_t lane_item) {
+  if (r == REG_HUB) return nchunks;
+  if (r == REG_LANE) return (cnt + 32 * lane_item - 1) / (32 * lane_item);
+  return (cnt * region_group(r) + 31) / 32;
+}
+// Batches of 32 one-lane vertices per work item. Each item is claimed with one atomic on the
+// launch-wide work counter: on low-degree graphs (tens of millions of one-lane vertices) items of
+// 4 batches keep that counter from serialising the iteration (2D lattice 2^25: 1.06 -> 0.89 ms
+// per iteration), while a graph with few one-lane vertices needs single batches to give every
+// resident warp work (R-MAT scale 16: 2.5x slower with 4). warps: resident warps of a launch.
+constexpr int LPA_WARPS_PER_SM = 24;  // lpa_run: 256-thread blocks, 3 resident per SM
+inline int64_t lane_item_for(int64_t lane_vertices, int64_t warps) {
+  const int64_t batches = (lane_vertices + 31) / 32, w = warps > 0 ? warps : 1;
+  return batches >= 32 * w ? 4 : batches >= 16 * w ? 2 : 1;
+}
+
 struct Regions {
   int64_t vbegin[NREG];
   int64_t vcount[NREG];
   int64_t ibegin[NREG + 1];  // item prefix; ibegin[NREG] = total items
+  int64_t lane_item;         // batches of 32 one-lane vertices per item (lane_item_for)
 };
 
 // Layout parameters (rak_options lane_max / hub_min / hub_chunk after defaults).
@@ -114,9 +133,14 @@ template <int S>
 cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, bool batch, cudaStream_t st, int *grid_out);
 template <int S>
 cudaError_t resolve_lpa_slots(int mode, bool off64, bool unit, bool batch, const void **fn, int *per_sm);
-// Whether neighbour marking inside work items reads each flag before storing it: measured to pay
-// for the Boyer-Moore sketch on graphs of 2^20 vertices and more, and to cost otherwise.
-inline int mark_test_for(int slots, int64_t n) { return slots == 1 && n >= (int64_t(1) << 20) ? 1 : 0; }
+// Whether neighbour marking inside work items reads each flag before storing it. Measured to pay
+// for the Boyer-Moore sketch on graphs of 2^20 vertices and more whose average degree is 8 or more
+// (R-MAT s22-s24: 25-35% faster; SBM 4M: 5%), where many moved vertices mark the same hub flags,
+// and to cost otherwise (2D lattices of degree ~4: 23-30% slower; small graphs, whose flags stay
+// in L1).
+inline int mark_test_for(int slots, int64_t n, int64_t m) {
+  return slots == 1 && n >= (int64_t(1) << 20) && m >= 8 * n ? 1 : 0;
+}
 // Loads and resolves the kernel a run will launch (outside its timed region).
 cudaError_t prepare_lpa(int slots, int mode, bool off64, bool unit, bool batch);
 

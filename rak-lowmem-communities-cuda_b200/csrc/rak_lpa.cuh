@@ -510,13 +510,17 @@ __global__ void __launch_bounds__(256, RAK_MIN_BLOCKS) lpa_run(const LpaArgs a) 
       while (item >= rg.ibegin[r + 1]) ++r;
       const int64_t local = item - rg.ibegin[r];
       if (r == REG_LANE) {
-        qn = lane_collect<S, MODE, O, UNIT, BATCH>(a, rg, local, vin, vout, fin, q, qn);
-        if (qn >= 32) {
-          RAK_BY_RULE(lane_batch, (a, g, q, 32, it, pickless, vin, vout, fin, fout, cnt));
-          __syncwarp();
-          if (lane < qn - 32) q[lane] = q[32 + lane];
-          __syncwarp();
-          qn -= 32;
+        for (int64_t sb = 0; sb < rg.lane_item; ++sb) {
+          const int64_t sub = local * rg.lane_item + sb;
+          if (sub * 32 >= rg.vcount[REG_LANE]) break;
+          qn = lane_collect<S, MODE, O, UNIT, BATCH>(a, rg, sub, vin, vout, fin, q, qn);
+          if (qn >= 32) {
+            RAK_BY_RULE(lane_batch, (a, g, q, 32, it, pickless, vin, vout, fin, fout, cnt));
+            __syncwarp();
+            if (lane < qn - 32) q[lane] = q[32 + lane];
+            __syncwarp();
+            qn -= 32;
+          }
         }
       } else if (r == REG_HUB) {
         RAK_BY_RULE(hub_item, (a, rg, g, local, it, pickless, vin, vout, fin, fout, cnt));

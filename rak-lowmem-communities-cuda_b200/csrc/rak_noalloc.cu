@@ -202,13 +202,16 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
     int64_t cnt[NREG] = {};
     for (int k = 0; k < 6; ++k) cnt[k] = int64_t(h[k]);
     for (int64_t k = 6; k < 6 + ly.lane_max; ++k) cnt[REG_LANE] += int64_t(h[k]);
+    int sms = 0;
+    NA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    rg.lane_item = lane_item_for(cnt[REG_LANE], int64_t(sms) * LPA_WARPS_PER_SM);
     int64_t v = 0, it = 0;
     for (int r = 0; r < NREG; ++r) {
       rg.vbegin[r] = v;
       rg.vcount[r] = cnt[r];
       v += cnt[r];
       rg.ibegin[r] = it;
-      it += r == REG_HUB ? nchunks : (cnt[r] * region_group(r) + 31) / 32;
+      it += region_items(r, cnt[r], nchunks, rg.lane_item);
     }
     rg.ibegin[NREG] = it;
   }
@@ -249,6 +252,7 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   a.pickless_step = o->pickless_step < 0 ? (mode == RAK_MODE_ASYNC ? 8 : 0) : o->pickless_step;
   a.check_on_pickless = o->check_on_pickless < 0 ? (mode == RAK_MODE_ASYNC ? 0 : 1) : (o->check_on_pickless ? 1 : 0);
   a.rescan = rescan;
+  a.mark_test = mark_test_for(slots, n, g->m);
   // rule sets as in rak_lowmem_cuda: the CPU rules unless sketch_rule asks for the GPU ones
   a.gpu_rule = mode != RAK_MODE_SYNC && o->sketch_rule == 2;
   a.timeout_ns = 20LL * 1000 * 1000 * 1000;
