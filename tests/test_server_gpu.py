@@ -54,16 +54,25 @@ def test_results_same_alone_and_in_the_mix(ctx):
     srv.close()
 
 
-def test_async_quality_in_the_mix(ctx):
+@pytest.mark.parametrize("label_order", [0, 2])
+def test_async_quality_in_the_mix(ctx, label_order):
+    """Default labels (ids) and the reference label order, rebuilt for every packed set of graphs;
+    a grid-numbered lattice in the mix finds its local structure with the reference order."""
     gs = [rl.gen_sbm(4000 + 1000 * k, 20, 16.0, 1000.0, seed=k) for k in range(8)]
-    srv = rl.Server(ctx, max_graphs_per_launch=3, slots=2)
+    lat = rl.gen_lattice(200, 150, 0.05, 0.01, seed=5)
+    srv = rl.Server(ctx, max_graphs_per_launch=3, slots=2, label_order=label_order)
     ts = [srv.submit(g) for g in gs]
+    tl = srv.submit(lat)
     import oracle as orc
     for t, g in zip(ts, gs):
         lab, res = srv.wait(t)
         assert lab.max() < g.n and res.iterations >= 1
         planted = orc.modularity(orc.Graph.of(g), g.truth)
         assert orc.modularity(orc.Graph.of(g), lab) >= 0.85 * planted
+    lab, res = srv.wait(tl)
+    assert lab.max() < lat.n
+    if label_order == 2:
+        assert orc.modularity(orc.Graph.of(lat), lab) > 0.4
     srv.close()
 
 
