@@ -418,8 +418,12 @@ def serving_leg(ctx, rates, seconds, threads, seed=11):
                 picks = np.where(rng.random(count) < 0.02, len(pool), rng.integers(0, len(pool), count))
                 srv = rl.Server(ctx, slots=2, validate=0)
                 # warm-up, untimed: grows both launch slots' pools and loads the kernels (the large
-                # graph twice at once, so each slot runs one; then pool graphs with and without it)
-                for ks in ([len(pool), len(pool)], [0, 1, 2, 3], [4, len(pool), 5]):
+                # graph twice at once, so each slot runs one; then pool graphs with and without it;
+                # then bursts of every graph, so launches of many graphs and every kernel size class
+                # have run before the timed arrivals -- the first process on a fresh machine
+                # otherwise pays lazy module loads from a cold file cache inside the arm)
+                burst = list(range(len(pool))) + [len(pool)]
+                for ks in ([len(pool), len(pool)], [0, 1, 2, 3], [4, len(pool), 5], burst, burst[::-1]):
                     for t in [(srv.submit_device(arena[k][1], arena[k][0]) if arm == "arena"
                                else srv.submit(graphs[k])) for k in ks]:
                         srv.wait(t, timeout=600.0)

@@ -234,13 +234,15 @@ typedef struct rak_tune_space {
   int32_t hub_chunk[8]; int32_t n_hub_chunk;  /* [2048 4096 8192 16384] */
   int32_t slots[5];     int32_t n_slots;      /* [4 8 16] */
   int32_t repeats;                            /* timed runs per candidate, best kept [2] */
-  int32_t reserved;
+  int32_t label_orders;                       /* 1: asynchronous runs also try the other label
+                                                 order (ids / reference order), first [1] */
   double quality_rel, quality_abs;            /* [0.005, 0.001] */
 } rak_tune_space;
 
 typedef struct rak_tune_entry {  /* one candidate that was run */
   int32_t lane_max, hub_min, hub_chunk, slots;
   int32_t iterations, accepted;  /* accepted: passed the quality gate */
+  int32_t label_order, reserved; /* label order of the run (1 ids, 2 reference order) */
   double ms;                     /* best time to result */
   double modularity;
   double edges_per_s;            /* traversed edges per second of that run */

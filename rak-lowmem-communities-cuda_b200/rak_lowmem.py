@@ -78,13 +78,14 @@ class rak_server_stats(C.Structure):
 class rak_tune_space(C.Structure):
     _fields_ = [("lane_max", C.c_int32 * 8), ("n_lane_max", C.c_int32), ("hub_min", C.c_int32 * 8),
                 ("n_hub_min", C.c_int32), ("hub_chunk", C.c_int32 * 8), ("n_hub_chunk", C.c_int32),
-                ("slots", C.c_int32 * 5), ("n_slots", C.c_int32), ("repeats", C.c_int32), ("reserved", C.c_int32),
+                ("slots", C.c_int32 * 5), ("n_slots", C.c_int32), ("repeats", C.c_int32), ("label_orders", C.c_int32),
                 ("quality_rel", C.c_double), ("quality_abs", C.c_double)]
 
 
 class rak_tune_entry(C.Structure):
     _fields_ = [("lane_max", C.c_int32), ("hub_min", C.c_int32), ("hub_chunk", C.c_int32), ("slots", C.c_int32),
-                ("iterations", C.c_int32), ("accepted", C.c_int32), ("ms", C.c_double), ("modularity", C.c_double),
+                ("iterations", C.c_int32), ("accepted", C.c_int32), ("label_order", C.c_int32),
+                ("reserved", C.c_int32), ("ms", C.c_double), ("modularity", C.c_double),
                 ("edges_per_s", C.c_double)]
 
 
@@ -197,7 +198,7 @@ def tune_space(**kw) -> rak_tune_space:
     return sp
 
 
-_OPTION_KEYS = ("lane_max", "hub_min", "hub_chunk", "slots")
+_OPTION_KEYS = ("lane_max", "hub_min", "hub_chunk", "slots", "label_order")
 
 
 def _tune_out(best, log, n):
@@ -492,8 +493,8 @@ class ResidentGraph:
         return _lib.rak_graph_device_bytes(self._g)
 
     def autotune(self, membership, space=None, **base_opts):
-        """rak_graph_autotune: returns ({lane_max, hub_min, hub_chunk, slots} of the best run, the
-        list of candidates run)."""
+        """rak_graph_autotune: returns ({lane_max, hub_min, hub_chunk, slots, label_order} of the best
+        run, the list of candidates run)."""
         o, best = options(**base_opts), rak_options()
         log, n = (rak_tune_entry * 64)(), C.c_int32(0)
         sp = space if space is not None else tune_space()

@@ -86,6 +86,9 @@ def test_tune_space_defaults():
     assert list(sp.hub_chunk)[:sp.n_hub_chunk] == [2048, 4096, 8192, 16384]
     assert list(sp.slots)[:sp.n_slots] == [4, 8, 16]
     assert sp.repeats == 2 and sp.quality_rel == 0.005 and sp.quality_abs == 0.001
+    assert sp.label_orders == 1
+    import ctypes
+    assert ctypes.sizeof(rl.rak_tune_entry) == 8 * 4 + 3 * 8      # label_order + reserved keep alignment
     sp = rl.tune_space(slots=[8], hub_chunk=[4096, 8192], repeats=1)
     assert sp.n_slots == 1 and sp.n_hub_chunk == 2 and sp.repeats == 1
     with pytest.raises(ValueError):

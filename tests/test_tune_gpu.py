@@ -21,6 +21,7 @@ def check_log(best, log, sp):
     for e in log[1:]:
         assert e["lane_max"] in list(sp.lane_max)[:sp.n_lane_max] + [start["lane_max"]]
         assert e["slots"] in list(sp.slots)[:sp.n_slots] + [start["slots"]]
+        assert e["label_order"] in (1, 2)
 
 
 def test_graph_autotune():
@@ -54,3 +55,19 @@ def test_batch_autotune():
         q = b.modularity(mem)
         assert np.all(np.asarray(q)[:6] > 0.5)
         b.close()
+
+
+def test_label_order_is_tuned_under_the_quality_gate():
+    """Both label orders are tried first; on a grid-numbered lattice id labels stall (the pickless
+    rule blocks the first moves) and fail the gate, so the reference order is kept."""
+    import torch
+    g = rl.gen_lattice(512, 512, 0.05, 0.01, seed=7)
+    sp = rl.tune_space(repeats=1, lane_max=[256], hub_min=[65536], hub_chunk=[8192], slots=[8])
+    with rl.Context(0) as ctx:
+        rg = rl.ResidentGraph(ctx, g)
+        mem = torch.empty(g.n, dtype=torch.int32, device="cuda")
+        best, log = rg.autotune(mem, space=sp)
+        check_log(best, log, sp)
+        assert log[0]["label_order"] == 2 and log[1]["label_order"] == 1
+        assert log[1]["accepted"] == 0 and best["label_order"] == 2
+        rg.close()
