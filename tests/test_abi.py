@@ -38,6 +38,8 @@ def test_option_defaults_follow_reference():
     # RakOptions defaults (inc/rak.hxx:37-38) and the reference's νMG8 choice (main.cxx:90).
     assert (o.repeat, o.tolerance, o.max_iterations, o.slots) == (1, 0.05, 20, 8)
     assert o.mode == rl.MODE_ASYNC and o.rescan == -1 and o.pickless_step == -1 and o.validate == 1
+    # rule set and label order resolve per mode and entry point (-1: the library's default)
+    assert o.sketch_rule == -1 and o.label_order == -1
 
 
 def test_no_device_reported_without_gpu():
