@@ -19,9 +19,10 @@ struct Sketch {
 // The two rule sets of the reference: its CPU code's (inc/rakLowmem.hxx) and its GPU code's
 // (inc/sketchCuda.hxx, inc/rakLowmemCuda.hxx). They differ in which free slot a new key takes,
 // whether decrements clamp at zero, how the argmax breaks ties, the Boyer-Moore starting candidate
-// and the weight test of the move rule. The synchronous modes follow the CPU rules (bit-exact
-// against the reference CPU code); the asynchronous mode follows the GPU rules, the path it
-// replaces.
+// and the weight test of the move rule. The synchronous exact mode follows the CPU rules (bit-exact
+// against the reference CPU code); the other modes run either set, chosen per launch (the CPU rules
+// by default: under the GPU rules' unclamped decrement R-MAT-like graphs collapse into one
+// community, as they do on the reference GPU path).
 enum : int { RULE_CPU = 1, RULE_GPU = 2 };
 
 // Cleared sketch. Boyer-Moore under the GPU rules starts from the vertex's own label d with weight

@@ -250,8 +250,8 @@ def test_device_csr_and_resident_runs(ctx):
 @pytest.mark.parametrize("slots", [8, 4, 1])
 @pytest.mark.parametrize("layout", [SMALL_LAYOUT, TINY_LAYOUT, None])
 def test_sync_split_gpu_rule_matches_oracle(ctx, name, slots, layout):
-    """The reference GPU sketch rules (the asynchronous mode's) checked bit for bit: the split
-    mode run with sketch_rule 2 against the oracle's restatement of those rules."""
+    """The reference GPU path's sketch rules checked bit for bit: the split mode run with
+    sketch_rule 2 against the oracle's restatement of those rules."""
     g = GRAPHS[name]
     lab, res = ctx.lowmem(g, mode=rl.MODE_SYNC_SPLIT, slots=slots, sketch_rule=2, **(layout or {}))
     ref, it, edges = orc.sync_run(orc.Graph.of(g), ocfg(slots, 0, split=1, layout=layout, gpu_rule=1))
