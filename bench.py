@@ -267,31 +267,49 @@ def nmi(a, b):
     return 1.0 if ha + hb == 0 else 2.0 * mi / (ha + hb)
 
 
-def batch_mix(count, seed, threads):
+def batch_mix(count, seed, threads, keep=None):
     """The batched-launch mix: vertex counts log-uniform in 2^10..2^18; half symmetric R-MAT
     (edge factor uniform in 8..32, power-of-two sizes), half planted-partition SBM (k uniform in
-    8..1024 equal blocks, clamped to n, average degree 16, p_in/p_out = 20); unit weights."""
+    8..1024 equal blocks, clamped to n, average degree 16, p_in/p_out = 20); unit weights.
+    keep(i) (optional) selects the graphs to build; every graph's parameters are still drawn, so
+    graph i is the same whichever subset is built."""
     import rak_lowmem as rl
     rng = np.random.default_rng(seed)
     graphs = []
     for i in range(count):
         if i % 2 == 0:
             scale = int(rng.integers(10, 19))
-            graphs.append(rl.gen_rmat(scale, float(rng.integers(8, 33)), seed=seed * 100003 + i, threads=threads))
+            ef = float(rng.integers(8, 33))
+            if keep is None or keep(i):
+                graphs.append(rl.gen_rmat(scale, ef, seed=seed * 100003 + i, threads=threads))
         else:
             n = int(round(2.0 ** rng.uniform(10, 18)))
             k = min(int(rng.integers(8, 1025)), n)
-            graphs.append(rl.gen_sbm(n, k, 16.0, 20.0, seed=seed * 100003 + i, threads=threads))
+            if keep is None or keep(i):
+                graphs.append(rl.gen_sbm(n, k, 16.0, 20.0, seed=seed * 100003 + i, threads=threads))
     return graphs
 
 
-def batched_leg(ctx, count, steps, threads, stream):
+def reduce_values(dist, values, op, device):
+    """all_reduce of a list of numbers (op: "max" or "sum"); without a process group, the values."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return [float(x) for x in t.tolist()]
+
+
+def batched_leg(ctx, count, steps, threads, stream, world=1, rank=0, dist=None):
     """Batched persistent launch (captured in a CUDA graph) vs a loop of plain per-graph runs on
-    resident graphs, same mix, same options; both timed on the device with CUDA events."""
+    resident graphs, same mix, same options; both timed on the device with CUDA events. With
+    several ranks the graphs are dealt round-robin (graph i to rank i mod N; independent graphs,
+    no collective on the data path) and the whole job is the slowest rank's time for all graphs."""
     import torch
     import rak_lowmem as rl
     t0 = time.time()
-    graphs = batch_mix(count, 4, threads)
+    graphs = batch_mix(count, 4, threads, keep=(lambda i: i % world == rank) if world > 1 else None)
+    mine = len(graphs)
     hb = rl.HostBatch.concat(graphs, weighted=False)
     log(f"[batched] {count} graphs, {hb.n} vertices, {hb.m} edges generated in {time.time() - t0:.1f}s")
     b = rl.Batch(ctx, hb)
@@ -314,7 +332,7 @@ def batched_leg(ctx, count, steps, threads, stream):
     off_d = torch.from_numpy(hb.offsets).cuda()
     tgt_d = torch.from_numpy(hb.targets.view(np.int32)).cuda()
     members, loop_out = [], []
-    for i in range(count):
+    for i in range(mine):
         a, z = int(hb.graph_offsets[i]), int(hb.graph_offsets[i + 1])
         e_a = int(hb.offsets[a])
         off_i = (off_d[a:z + 1] - e_a).contiguous()
@@ -346,7 +364,13 @@ def batched_leg(ctx, count, steps, threads, stream):
     for _, rg in members:
         rg.close()
     b.close()
-    return {"graphs": count, "vertices": int(hb.n), "edges": int(hb.m),
+    # whole job over ranks (every rank takes these steps in this order)
+    t_batch, t_loop, it_max = reduce_values(dist, [t_batch, t_loop, int(iters.max())], "max", "cuda")
+    sums = reduce_values(dist, [mine, hb.n, hb.m, tot.traversed_edges, float(np.sum(q_batch)), float(np.sum(q_loop)),
+                                float(np.sum(nmis)), len(nmis), float(np.sum(nmis_loop))], "sum", "cuda")
+    count, n_all, m_all, trav, qb_sum, ql_sum, nmi_sum, nmi_cnt, nmil_sum = sums
+    count = int(count)
+    return {"graphs": count, "vertices": int(n_all), "edges": int(m_all),
             "mix": "half symmetric R-MAT (ef U{8..32}, n = 2^U{10..18}), half planted SBM (k U{8..1024}, "
                    "avg degree 16, p_in/p_out 20, n log-uniform 2^10..2^18), unit weights, seed 4",
             "graphs_per_s": count / t_batch, "ms_per_batch": 1e3 * t_batch,
@@ -354,10 +378,12 @@ def batched_leg(ctx, count, steps, threads, stream):
             "batched_path": "rak_batch_capture + rak_batch_replay (one persistent launch in a CUDA graph)",
             "loop_path": "rak_graph_run per resident graph (one persistent launch + read-back each), labels by "
                          "vertex id as the batch's default (label_order 1)",
-            "edges_per_s": tot.traversed_edges / t_batch, "iterations_max": int(iters.max()),
-            "modularity_mean": float(np.mean(q_batch)), "loop_modularity_mean": float(np.mean(q_loop)),
-            "nmi_sbm_mean": float(np.mean(nmis)) if nmis else None,
-            "loop_nmi_sbm_mean": float(np.mean(nmis_loop)) if nmis_loop else None}
+            "edges_per_s": trav / t_batch, "iterations_max": int(it_max),
+            "modularity_mean": qb_sum / count, "loop_modularity_mean": ql_sum / count,
+            "nmi_sbm_mean": nmi_sum / nmi_cnt if nmi_cnt else None,
+            "loop_nmi_sbm_mean": nmil_sum / nmi_cnt if nmi_cnt else None,
+            "sharding": (f"graphs dealt round-robin to {world} ranks (no collective on the data path); times are "
+                         "the slowest rank's" if world > 1 else "single GPU")}
 
 
 def serving_leg(ctx, rates, seconds, threads, seed=11):
@@ -505,6 +531,8 @@ def main():
         ap.error("--warmup must be >= 3")
     spec = WORKLOADS[args.workload]
     world, rank, local = dist_setup()
+    if 0 < args.batch_graphs < world:
+        ap.error("--batch-graphs must be at least the number of ranks (graphs are dealt to ranks)")
     if args.impl == "reference":
         run_reference(args, spec, world, rank)
         return
@@ -646,7 +674,7 @@ def main():
         cpu_gve = cpu_baseline_gve(g)
     batched = None
     if args.batch_graphs > 0:
-        batched = batched_leg(ctx, args.batch_graphs, 3, threads, stream)
+        batched = batched_leg(ctx, args.batch_graphs, 3, threads, stream, world, rank, pg)
     serving = None
     if args.serving_seconds > 0 and world == 1:
         serving = serving_leg(ctx, [int(x) for x in args.serving_rates.split(",")], args.serving_seconds, threads)

@@ -60,3 +60,19 @@ def test_single_process_is_local():
     sys.path.insert(0, ROOT)
     import bench
     assert bench.whole_job(None, 2.5, 7, "cpu") == (2.5, 7.0)
+
+
+def test_batch_mix_shares_are_the_full_mix():
+    """The batched leg deals graph i to rank i mod N: each rank's share, built on its own, is the
+    same graphs as those positions of the full mix."""
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    import bench
+    full = bench.batch_mix(6, 4, 4)
+    for rank in range(2):
+        part = bench.batch_mix(6, 4, 4, keep=lambda i: i % 2 == rank)
+        assert len(part) == 3
+        for j, g in enumerate(part):
+            f = full[2 * j + rank]
+            np.testing.assert_array_equal(g.offsets, f.offsets)
+            np.testing.assert_array_equal(g.targets, f.targets)
