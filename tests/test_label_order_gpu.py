@@ -103,3 +103,21 @@ def test_batched_lattice_does_not_stall(ctx, slots):
         assert q[i] == pytest.approx(orc.modularity(orc.Graph.of(g), lab[a:z]), rel=1e-9, abs=1e-12)
     assert q[0] > 0.4 and q[2] > 0.4, q
     b.close()
+
+
+@pytest.mark.parametrize("rule", [1, 2])
+@pytest.mark.parametrize("name", ["rmat12", "lattice"])
+def test_sync_split_from_reference_positions_matches_oracle(ctx, rule, name):
+    """The reference label order run deterministically: the synchronous split mode started from the
+    reference's positions as initial labels (q) -- the labels the pickless rule then compares --
+    equals the oracle's synchronous run from the same labels, bit for bit, under either rule set."""
+    g = rl.gen_rmat(12, 8, seed=21) if name == "rmat12" else rl.gen_lattice(120, 90, 0.05, 0.01, seed=22)
+    ks = orc.ref_vertex_order(g)
+    pos = np.empty_like(ks)
+    pos[ks] = np.arange(len(ks), dtype=np.uint32)
+    lab, res = ctx.lowmem(g, q=pos, mode=rl.MODE_SYNC_SPLIT, sketch_rule=rule)
+    o = orc.make_opts(slots=8, rescan=0, split=1, layout=orc.DEFAULT_LAYOUT, gpu_rule=1 if rule == 2 else 0)
+    ref, it, edges = orc.sync_run(orc.Graph.of(g), o, q=pos)
+    assert res.iterations == it
+    np.testing.assert_array_equal(lab, ref)
+    assert res.traversed_edges == edges
