@@ -22,6 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_CPU_SO = os.path.join(HERE, "_ref", "libref_cpu.so")
 REF_CUDA_BIN = os.path.join(HERE, "_ref", "ref_lpa_cuda")
+REF_SKETCH_BIN = os.path.join(HERE, "_ref", "ref_sketch_cuda")
 NONE = 0xFFFFFFFF
 MAX_SLOTS = 32
 
@@ -306,3 +307,39 @@ def ref_lowmem_cuda(g, slots=8, repeat=1, tolerance=0.05, max_iterations=20, tim
         info = json.loads(p.stdout.strip().splitlines()[-1])
         labels = np.fromfile(lp, dtype=np.uint32)
     return labels, info
+
+
+def have_ref_sketch_cuda() -> bool:
+    return os.path.exists(REF_SKETCH_BIN)
+
+
+def ref_sketch_streams_gpu(slots, streams, timeout=120):
+    """The reference's own GPU Misra-Gries accumulate and tournament argmax (inc/sketchCuda.hxx,
+    sketchAccumulateWarpCudU and sketchMaxGroupReduceCudU) on each stream of (community, weight)
+    pairs, from cleared keys: per stream the slots [(key, weight)] before the argmax and the
+    (key, weight) it picks. Runs oracle/_ref/ref_sketch_cuda as a separate process."""
+    off = np.zeros(len(streams) + 1, np.int64)
+    off[1:] = np.cumsum([len(st) for st in streams])
+    comm = np.array([c for st in streams for c, _ in st], np.uint32)
+    wts = np.array([w for st in streams for _, w in st], np.float32)
+    ns, total = len(streams), int(off[-1])
+    with tempfile.TemporaryDirectory() as d:
+        ip, op = os.path.join(d, "s.in"), os.path.join(d, "s.out")
+        with open(ip, "wb") as f:
+            f.write(b"RAKSKT01")
+            f.write(np.array([slots], np.int32).tobytes())
+            f.write(np.array([ns, total], np.int64).tobytes())
+            f.write(off.tobytes())
+            f.write(comm.tobytes())
+            f.write(wts.tobytes())
+        p = subprocess.run([REF_SKETCH_BIN, ip, op], capture_output=True, text=True, timeout=timeout)
+        if p.returncode != 0:
+            raise RuntimeError(f"ref_sketch_cuda failed ({p.returncode}): {p.stderr[-2000:]}")
+        raw = open(op, "rb").read()
+    nk = ns * slots
+    keys = np.frombuffer(raw, np.uint32, nk, 0).reshape(ns, slots)
+    ws = np.frombuffer(raw, np.float32, nk, 4 * nk).reshape(ns, slots)
+    bk = np.frombuffer(raw, np.uint32, ns, 8 * nk)
+    bw = np.frombuffer(raw, np.float32, ns, 8 * nk + 4 * ns)
+    return [([(int(keys[i, j]), float(ws[i, j])) for j in range(slots)], (int(bk[i]), float(bw[i])))
+            for i in range(ns)]
