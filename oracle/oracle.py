@@ -313,11 +313,13 @@ def have_ref_sketch_cuda() -> bool:
     return os.path.exists(REF_SKETCH_BIN)
 
 
-def ref_sketch_streams_gpu(slots, streams, timeout=120):
+def ref_sketch_streams_gpu(slots, streams, own=None, timeout=120):
     """The reference's own GPU Misra-Gries accumulate and tournament argmax (inc/sketchCuda.hxx,
     sketchAccumulateWarpCudU and sketchMaxGroupReduceCudU) on each stream of (community, weight)
     pairs, from cleared keys: per stream the slots [(key, weight)] before the argmax and the
-    (key, weight) it picks. Runs oracle/_ref/ref_sketch_cuda as a separate process."""
+    (key, weight) it picks. slots 1: the reference's Boyer-Moore scan
+    (rakLowmemBmScanCommunitiesCud) from own[i], the own label of stream i's vertex. Runs
+    oracle/_ref/ref_sketch_cuda as a separate process."""
     off = np.zeros(len(streams) + 1, np.int64)
     off[1:] = np.cumsum([len(st) for st in streams])
     comm = np.array([c for st in streams for c, _ in st], np.uint32)
@@ -332,6 +334,8 @@ def ref_sketch_streams_gpu(slots, streams, timeout=120):
             f.write(off.tobytes())
             f.write(comm.tobytes())
             f.write(wts.tobytes())
+            if slots == 1:
+                f.write(np.asarray(own, np.uint32).tobytes())
         p = subprocess.run([REF_SKETCH_BIN, ip, op], capture_output=True, text=True, timeout=timeout)
         if p.returncode != 0:
             raise RuntimeError(f"ref_sketch_cuda failed ({p.returncode}): {p.stderr[-2000:]}")

@@ -1,6 +1,8 @@
 """The oracle's restatement of the reference GPU sketch rules (a new key takes the first free slot,
-a full sketch decrements without clamping, the argmax is a tournament) against the reference's
-own device functions (inc/sketchCuda.hxx: sketchAccumulateWarpCudU, sketchMaxGroupReduceCudU),
+a full sketch decrements without clamping, the argmax is a tournament; Boyer-Moore starts from the
+vertex's own label) against the reference's own device functions (inc/sketchCuda.hxx:
+sketchAccumulateWarpCudU, sketchMaxGroupReduceCudU; inc/rakLowmemCuda.hxx:
+rakLowmemBmScanCommunitiesCud),
 compiled from its sources into oracle/_ref and run on the GPU on the same streams: every slot and
 the chosen (key, weight) must be identical. Weights are multiples of 0.5, so sums and differences
 are exact, and include zero weights, exact decrements to zero and ties."""
@@ -35,3 +37,16 @@ def test_gpu_rule_sketch_matches_reference_device_code(slots):
             s.add(c, w)
         assert s.slots_list() == ref_slots, (i, st)
         assert s.choose() == ref_best, (i, st)
+
+
+def test_gpu_rule_boyer_moore_matches_reference_device_code():
+    sts = streams(1, 3000, 7)
+    rng = np.random.default_rng(8)
+    own = rng.integers(0, 4, len(sts)).tolist()
+    got = orc.ref_sketch_streams_gpu(1, sts, own=own)
+    for i, (st, d, (ref_slots, ref_best)) in enumerate(zip(sts, own, got)):
+        s = orc.Sketch(1, gpu_rule=True)
+        s.s.k[0], s.s.w[0] = d, 0.0                   # the GPU rules start from the own label
+        for c, w in st:
+            s.add(c, w)
+        assert s.slots_list()[0] == ref_best == ref_slots[0], (i, d, st)
