@@ -4,6 +4,8 @@
 - _ref/libref_cpu.so: the reference's own CPU code compiled from its sources (ref_bridge.cpp);
   present only where the reference sources were available at build time.
 - _ref/ref_lpa_cuda: the reference's own GPU path as a separate program (ref_main_cuda.cu).
+- _ref/ref_sketch_cuda: the reference's own GPU sketch device functions on given streams, as a
+  separate program (ref_sketch_cuda.cu), the pin of the GPU-rule restatement.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module, and only as
 the checker or the CPU baseline; the product never imports it.
