@@ -40,6 +40,30 @@ int main() {
     std::printf("thresholds\n");
     return 1;
   }
+  // plan keys: every degree maps into the histogram's range and to its region -- one lane up to
+  // lane_max, split vertices above hub_min, else the smallest group G >= 2 (power of two, <= 32)
+  // with G * lane_max >= degree
+  const rak::Layout layouts[] = {{256, 65536, 8192}, {8, 64, 32}, {128, 8192, 4096}, {1, 1, 32}, {32, 4096, 2048}};
+  for (const rak::Layout &ly : layouts) {
+    const int64_t nkeys = 6 + ly.lane_max + 1;
+    for (int64_t deg = 0; deg <= 2 * ly.hub_min + 10; ++deg) {
+      const uint32_t k = rak::plan_key(deg, ly);
+      const int r = rak::key_region(k);
+      bool ok = int64_t(k) < nkeys;
+      if (deg == 0) ok = ok && int64_t(k) == nkeys - 1;
+      else if (deg <= ly.lane_max) ok = ok && r == rak::REG_LANE;
+      else if (deg > ly.hub_min) ok = ok && r == rak::REG_HUB;
+      else {
+        const int64_t G = rak::region_group(r);
+        ok = ok && r >= 1 && r <= 5 && (G * ly.lane_max >= deg || G == 32) && (G == 2 || (G / 2) * ly.lane_max < deg);
+      }
+      if (!ok) {
+        std::printf("plan_key(%lld) = %u, region %d (layout %lld/%lld)\n", (long long)deg, k, r,
+                    (long long)ly.lane_max, (long long)ly.hub_min);
+        return 1;
+      }
+    }
+  }
   std::printf("ok\n");
   return 0;
 }

@@ -1,7 +1,9 @@
-"""The one-lane work-item arithmetic of the plan (rak_internal.hpp: lane_item_for, region_items)
-and the kernel's loop over an item's batches visit every one-lane vertex exactly once, for region
-sizes 0..20000 and grids of 1 to 100000 warps; checked on the host by compiling the library's own
-header (tests/cpp/plan_items.cpp)."""
+"""The plan's arithmetic, checked on the host by compiling the library's own header
+(rak_internal.hpp) into tests/cpp/plan_items.cpp: the one-lane work items (lane_item_for,
+region_items) and the kernel's loop over an item's batches visit every one-lane vertex exactly
+once, for region sizes 0..20000 and grids of 1 to 100000 warps; and plan_key maps every degree into
+the key histogram's range and to its region (one lane, the smallest sufficient lane group, or
+split) for five layouts."""
 import os
 import subprocess
 
