@@ -55,3 +55,24 @@ def test_segmented_order_equals_reference_partition():
     for i, g in enumerate(gs):
         a, z = int(hb.graph_offsets[i]), int(hb.graph_offsets[i + 1])
         np.testing.assert_array_equal(ks[a:z], orc.ref_vertex_order(g), err_msg=f"graph {i}")
+
+
+def test_segmented_order_on_random_degree_sequences():
+    """Batches of random graphs whose degrees straddle both partition limits (< 4 and < 128)."""
+    rng = np.random.default_rng(1234)
+    for trial in range(20):
+        gs = []
+        for _ in range(int(rng.integers(1, 6))):
+            n = int(rng.integers(1, 400))
+            kind = rng.random(n)
+            deg = np.where(kind < 0.4, rng.integers(0, 4, n), np.where(kind < 0.9, rng.integers(4, 128, n),
+                                                                       rng.integers(128, 200, n)))
+            off = np.zeros(n + 1, np.int64)
+            off[1:] = np.cumsum(deg)
+            tgt = rng.integers(0, n, int(off[-1])).astype(np.uint32)    # any targets: only degrees matter
+            gs.append(rl.HostGraph(off, tgt))
+        hb = rl.HostBatch.concat(gs)
+        ks = segmented_order(np.asarray(hb.offsets), np.asarray(hb.graph_offsets))
+        for i, g in enumerate(gs):
+            a, z = int(hb.graph_offsets[i]), int(hb.graph_offsets[i + 1])
+            np.testing.assert_array_equal(ks[a:z], orc.ref_vertex_order(g), err_msg=f"trial {trial} graph {i}")
