@@ -17,6 +17,7 @@ import json
 import os
 import subprocess
 import tempfile
+import weakref
 
 import numpy as np
 
@@ -25,6 +26,7 @@ ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_CPU_SO = os.path.join(HERE, "_ref", "libref_cpu.so")
 REF_CUDA_BIN = os.path.join(HERE, "_ref", "ref_lpa_cuda")
 REF_SKETCH_BIN = os.path.join(HERE, "_ref", "ref_sketch_cuda")
+GEN_SO = os.path.join(HERE, "liborcgen.so")
 NONE = 0xFFFFFFFF
 MAX_SLOTS = 32
 
@@ -33,7 +35,7 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
-if not os.path.exists(ORACLE_SO):
+if not os.path.exists(ORACLE_SO) or not os.path.exists(GEN_SO):
     build()
 _o = C.CDLL(ORACLE_SO)
 
@@ -91,6 +93,7 @@ class Graph:
         self.targets = np.ascontiguousarray(targets, dtype=np.uint32)
         self.weights = None if weights is None else np.ascontiguousarray(weights, dtype=np.float32)
         self.n = len(self.offsets) - 1
+        self.m = len(self.targets)
         self.c = orc_csr(self.n, self.offsets.ctypes.data, self.targets.ctypes.data if len(self.targets) else None,
                          self.weights.ctypes.data if self.weights is not None else None)
 
@@ -180,6 +183,50 @@ class Sketch:
         return [(int(self.s.k[i]), float(self.s.w[i])) for i in range(self.slots)]
 
 
+# ---- the library's synthetic graphs, restated (rmat_gen.c) -----------------------------------
+class og_graph(C.Structure):
+    _fields_ = [("n", C.c_int64), ("m", C.c_int64), ("off", P), ("tgt", P), ("wt", P)]
+
+
+_gen = C.CDLL(GEN_SO)
+_sig(_gen, "og_gen_rmat", C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_float,
+     C.c_float, C.c_int, C.POINTER(og_graph))
+_sig(_gen, "og_gen_lattice", C.c_int, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_uint64, C.c_int,
+     C.POINTER(og_graph))
+_sig(_gen, "og_free", None, C.POINTER(og_graph))
+
+
+def _take(og: og_graph) -> Graph:
+    """A Graph whose arrays view the generated C arrays (no copy: a scale-27 graph is ~17 GB); the
+    C arrays are freed when the Graph is collected, so keep the Graph while its arrays are used."""
+    n, m = int(og.n), int(og.m)
+    off = np.ctypeslib.as_array(C.cast(og.off, C.POINTER(C.c_int64)), shape=(n + 1,))
+    tgt = np.ctypeslib.as_array(C.cast(og.tgt, C.POINTER(C.c_uint32)), shape=(max(m, 1),))[:m]
+    wt = np.ctypeslib.as_array(C.cast(og.wt, C.POINTER(C.c_float)), shape=(max(m, 1),))[:m] if og.wt else None
+    g = Graph(off, tgt, wt)
+    g._owner = og
+    weakref.finalize(g, _gen.og_free, C.byref(og))
+    return g
+
+
+def gen_rmat(scale, edge_factor, a=0.57, b=0.19, c=0.19, seed=42, w_lo=1.0, w_hi=1.0, threads=0) -> Graph:
+    """The library's symmetric R-MAT (rak_gen_rmat), restated in C: bit-identical arrays."""
+    og = og_graph()
+    st = _gen.og_gen_rmat(scale, edge_factor, a, b, c, seed, w_lo, w_hi, threads, C.byref(og))
+    if st:
+        raise RuntimeError(f"og_gen_rmat failed ({st})")
+    return _take(og)
+
+
+def gen_lattice(width, height, p_delete=0.05, shortcut=0.01, seed=42, threads=0) -> Graph:
+    """The library's perturbed 2D lattice (rak_gen_lattice), restated in C: bit-identical arrays."""
+    og = og_graph()
+    st = _gen.og_gen_lattice(width, height, p_delete, shortcut, seed, threads, C.byref(og))
+    if st:
+        raise RuntimeError(f"og_gen_lattice failed ({st})")
+    return _take(og)
+
+
 # ---- the reference itself, compiled from its sources ------------------------------------------
 _ref = None
 
@@ -196,6 +243,9 @@ def ref_cpu():
         _ref = C.CDLL(REF_CPU_SO)
         _sig(_ref, "ref_lowmem_omp", C.c_int, C.c_int64, P, P, P, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
              C.c_int, P, C.POINTER(C.c_float))
+        _sig(_ref, "ref_lowmem_omp_sample", C.c_int64, C.c_int64, P, P, P, C.c_int, C.c_int, C.c_int64, C.c_int,
+             C.POINTER(C.c_float))
+        _sig(_ref, "ref_gve_omp_sample", C.c_int64, C.c_int64, P, P, P, C.c_int64, C.c_int, C.POINTER(C.c_float))
         _sig(_ref, "ref_gve_omp", C.c_int, C.c_int64, P, P, P, C.c_double, C.c_int, C.c_int, C.c_int, P,
              C.POINTER(C.c_float))
         _sig(_ref, "ref_modularity", C.c_double, C.c_int64, P, P, P, P)
@@ -254,6 +304,27 @@ def ref_lowmem_omp(g, slots=8, rescan=1, tolerance=0.05, max_iterations=20, thre
     if it < 0:
         raise ValueError(f"unsupported slots {slots}")
     return out, int(it), float(t.value)
+
+
+def ref_lowmem_omp_sample(g, slots=8, rescan=1, stride=1, threads=1):
+    """One first iteration of the reference's rakLowmemInvokeOmp<MULTI,RESCAN,SLOTS> with
+    rakLowmemStaticOmp's hooks, restricted to every stride-th vertex (inc/rakLowmem.hxx:226-284).
+    Returns (traversed edges, the reference's own time in ms)."""
+    g = Graph.of(g)
+    t = C.c_float(0)
+    e = ref_cpu().ref_lowmem_omp_sample(*_gp(g), slots, rescan, stride, threads, C.byref(t))
+    if e < 0:
+        raise ValueError(f"unsupported slots {slots}")
+    return int(e), float(t.value)
+
+
+def ref_gve_omp_sample(g, stride=1, threads=1):
+    """The same sample of GVE-LPA's first iteration (rakInvokeOmp with rakStaticOmp's hooks,
+    inc/rak.hxx:272-327). Returns (traversed edges, time in ms)."""
+    g = Graph.of(g)
+    t = C.c_float(0)
+    e = ref_cpu().ref_gve_omp_sample(*_gp(g), stride, threads, C.byref(t))
+    return int(e), float(t.value)
 
 
 def ref_gve_omp(g, tolerance=0.05, max_iterations=20, threads=1, repeat=1):

@@ -142,6 +142,56 @@ int ref_gve_omp(int64_t n, const int64_t *off, const uint32_t *tgt, const float 
   return r.iterations;
 }
 
+// A bounded sample of the reference's first iteration, for timing on the host cores: its own setup
+// function rakLowmemInvokeOmp<MULTI,RESCAN,SLOTS> (inc/rakLowmem.hxx:226-262) with the hooks of
+// rakLowmemStaticOmp (:277-284: labels initialised by rakInitializeOmpW, every vertex marked
+// affected) except that the "is vertex allowed to be updated" hook admits every stride-th vertex
+// (0-based ids 0, stride, 2*stride, ...), and one iteration. Returns the traversed edges (the
+// admitted vertices' degrees, summed outside the timed region); *time_ms is the reference's own
+// measureDuration of the run. -1 for an unsupported slot count.
+int64_t ref_lowmem_omp_sample(int64_t n, const int64_t *off, const uint32_t *tgt, const float *wt, int slots,
+                              int rescan, int64_t stride, int threads, float *time_ms) {
+  if (threads > 0) omp_set_num_threads(threads);
+  if (stride < 1) stride = 1;
+  ShiftedCsr x{n, off, tgt, wt};
+  int64_t edges = 0;
+  for (int64_t u = 0; u < n; u += stride) edges += off[u + 1] - off[u];
+  const RakOptions o(1, 0.0, 1);
+  using FLAG = char;
+  auto fi = [&](auto &vcom) { rakInitializeOmpW(vcom, x); };
+  auto fm = [](auto &vaff, auto &vcs, auto &vcout, const auto &vcom) { fillValueOmpU(vaff, FLAG(1)); };
+  auto fa = [=](auto u) { return (int64_t(u) - 1) % stride == 0; };
+  float t = -1;
+  if (slots == 1) t = rakLowmemInvokeOmp<false, false, 8>(x, o, fi, fm, fa).time;
+#define RS(S)                                                                 \
+  else if (slots == S) t = rescan ? rakLowmemInvokeOmp<true, true, S>(x, o, fi, fm, fa).time \
+                                  : rakLowmemInvokeOmp<true, false, S>(x, o, fi, fm, fa).time;
+  RS(2) RS(4) RS(8) RS(16) RS(32)
+#undef RS
+  else return -1;
+  if (time_ms) *time_ms = t;
+  return edges;
+}
+
+// The same bounded sample of GVE-LPA's first iteration: rakInvokeOmp (inc/rak.hxx:272-310) with the
+// hooks of rakStaticOmp (:320-327) except for the same every-stride-th-vertex "allowed" hook.
+int64_t ref_gve_omp_sample(int64_t n, const int64_t *off, const uint32_t *tgt, const float *wt, int64_t stride,
+                           int threads, float *time_ms) {
+  if (threads > 0) omp_set_num_threads(threads);
+  if (stride < 1) stride = 1;
+  ShiftedCsr x{n, off, tgt, wt};
+  int64_t edges = 0;
+  for (int64_t u = 0; u < n; u += stride) edges += off[u + 1] - off[u];
+  const RakOptions o(1, 0.0, 1);
+  using FLAG = char;
+  auto fi = [&](auto &vcom) { rakInitializeOmpW(vcom, x); };
+  auto fm = [](auto &vaff, auto &vcs, auto &vcout, const auto &vcom) { fillValueOmpU(vaff, FLAG(1)); };
+  auto fa = [=](auto u) { return (int64_t(u) - 1) % stride == 0; };
+  const float t = rakInvokeOmp(x, o, fi, fm, fa).time;
+  if (time_ms) *time_ms = t;
+  return edges;
+}
+
 // modularityBy (inc/properties.hxx:177-192) with M = edgeWeightOmp(x)/2 as main.cxx:61 does.
 double ref_modularity(int64_t n, const int64_t *off, const uint32_t *tgt, const float *wt,
                       const uint32_t *labels) {
