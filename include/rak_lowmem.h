@@ -103,8 +103,14 @@ typedef struct rak_options {
                                  rule compares; results are vertex ids either way; in a batch,
                                  each graph's own order. Single-graph ASYNC runs: 2 [2]; batches
                                  and the server: 1 [1], 2 on request; SYNC modes: 1 only. Graph
-                                 steps and the no-alloc entry label by id and refuse 2 */
-  int64_t reserved[7];
+                                 steps label by id and refuse 2 */
+  int64_t wait_timeout_ns;    /* 0: default [20 s]; bound on each device-side wait (the grid barrier
+                                 between iterations). When it runs out the launch records
+                                 RAK_ERR_TIMEOUT, every block leaves, and the call returns that
+                                 status with the context still usable (the reference has no bound:
+                                 a stuck kernel hangs its blocking read-back, inc/rakLowmemCuda.hxx
+                                 :486, and errors exit(), inc/_cuda.hxx:221-235) */
+  int64_t reserved[6];
 } rak_options;
 
 typedef struct rak_result {
@@ -324,13 +330,17 @@ rak_status rak_server_destroy(rak_server *s);
  * RAK_NOALLOC_SCRATCH_BYTES; it calls no cudaMalloc, cudaFree or allocating library routine.
  * g, q (may be NULL), o->initial_flags (may be NULL) and membership are device pointers; work is
  * issued on `stream` (a cudaStream_t, NULL = legacy default stream) of `device`.
- * Graphs whose buffers exceed the array (roughly 20 bytes per vertex, plus 8*slots bytes per
- * split chunk) return RAK_ERR_OUT_OF_MEMORY with res->peak_device_bytes set to the bytes needed.
+ * Graphs whose buffers exceed the array (roughly 20 bytes per vertex, 28 with the reference label
+ * order that asynchronous runs use by default, plus 8*slots bytes per split chunk) return
+ * RAK_ERR_OUT_OF_MEMORY with res->peak_device_bytes set to the bytes needed. Options and labels
+ * mean what they mean for rak_lowmem_cuda.
  * The first call on a device looks the array up on that device (make it before any stream
- * capture). All calls share the array and it keeps the last call's contents; each call clears
- * what must start at zero, and calls that overlap on the GPU race on it. Times in res are host
- * wall-clock (no CUDA events are created). Labels are vertex ids in every mode: label_order 2
- * returns RAK_ERR_UNSUPPORTED. */
+ * capture). CUDA places the array, and each kernel variant's code (slot count, mode, offset width,
+ * weighted or unit), on a device lazily, when a call first needs it; those are the runtime's own
+ * device allocations, so a caller about to hand a device's memory to a pool makes one call of each
+ * variant it will use first. All calls share the array and it keeps the last call's contents; each
+ * call clears what must start at zero, and calls that overlap on the GPU race on it. Times in res
+ * are host wall-clock (no CUDA events are created). The caller's current device is restored. */
 rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const rak_csr *g, const uint32_t *q,
                                    const rak_options *o, uint32_t *membership, rak_result *res);
 

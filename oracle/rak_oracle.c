@@ -207,6 +207,9 @@ uint64_t orc_sync_step(const orc_csr *g, const orc_opts *o, int iteration,
   uint64_t changed = 0, edges = 0, processed = 0;
   memset(aff_next, 0, (size_t)g->n);
   for (int64_t u = 0; u < g->n; ++u) vcom_next[u] = vcom_prev[u];
+  /* Every decision reads only the snapshot, so vertices are independent and may be decided by
+   * several threads (OpenMP; one thread gives the same result). Marks are idempotent stores. */
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : changed, edges, processed)
   for (int64_t u = 0; u < g->n; ++u) {
     if (!aff_prev[u]) continue;
     int64_t deg = g->off[u + 1] - g->off[u];
@@ -220,7 +223,7 @@ uint64_t orc_sync_step(const orc_csr *g, const orc_opts *o, int iteration,
     if (pl && c > d) continue;
     vcom_next[u] = c; ++changed;
     for (int64_t e = g->off[u]; e < g->off[u + 1]; ++e)
-      if (g->tgt[e] != (uint32_t)u) aff_next[g->tgt[e]] = 1;
+      if (g->tgt[e] != (uint32_t)u) __atomic_store_n(&aff_next[g->tgt[e]], (uint8_t)1, __ATOMIC_RELAXED);
   }
   if (edges_out) *edges_out += edges;
   if (processed_out) *processed_out += processed;

@@ -57,6 +57,8 @@ constexpr int64_t DEFAULT_LANE_MAX = 256;
 constexpr int64_t DEFAULT_HUB_MIN = 65536;
 constexpr int64_t DEFAULT_HUB_CHUNK = 8192;
 constexpr int64_t MAX_LANE_MAX = 1024;
+// Bound on each device-side wait when rak_options.wait_timeout_ns is 0.
+constexpr long long DEFAULT_WAIT_TIMEOUT_NS = 20LL * 1000 * 1000 * 1000;
 
 // Sort key of a vertex in the plan (regions in order, region 6 by degree descending);
 // key_isolated for degree 0. Shared by the device plan kernel and the host summary.

@@ -45,10 +45,41 @@ struct G_ {
   const float *wt;
 };
 
+// Edge-stream loads (targets, weights). An iteration reads each of them once, so they carry an L2
+// evict-first cache policy (an operand of the load instruction, not a setting of the GPU): the L2's
+// capacity stays with the neighbour-label gathers, which repeat (a label is read once per incident
+// edge). RAK_STREAM_HINT=0 compiles plain non-coherent loads instead.
+#ifndef RAK_STREAM_HINT
+#define RAK_STREAM_HINT 1
+#endif
+__device__ __forceinline__ uint64_t l2_stream_policy() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint32_t ld_edge(const uint32_t *p) {
+#if RAK_STREAM_HINT
+  uint32_t v;
+  asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(l2_stream_policy()));
+  return v;
+#else
+  return __ldg(p);
+#endif
+}
+__device__ __forceinline__ float ld_weight(const float *p) {
+#if RAK_STREAM_HINT
+  float v;
+  asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(l2_stream_policy()));
+  return v;
+#else
+  return __ldg(p);
+#endif
+}
+
 template <bool UNIT>
 __device__ __forceinline__ float edge_w(const float *wt, int64_t e) {
   if constexpr (UNIT) return 1.0f;
-  else return __ldg(wt + e);
+  else return ld_weight(wt + e);
 }
 
 // Sequential sketch of edges e, e+st, ... < ee of u (self-loops skipped), in edge order.
@@ -66,7 +97,7 @@ __device__ __forceinline__ void scan_range(Sketch<S> &sk, uint32_t u, int64_t e,
 #pragma unroll
   for (int j = 0; j < B; ++j) {
     const int64_t x = e + int64_t(j) * st;
-    t[j] = x < ee ? base + __ldg(tgt + x) : u;
+    t[j] = x < ee ? base + ld_edge(tgt + x) : u;
     w[j] = x < ee ? edge_w<UNIT>(wt, x) : 0.0f;
   }
   while (e < ee) {
@@ -79,7 +110,7 @@ __device__ __forceinline__ void scan_range(Sketch<S> &sk, uint32_t u, int64_t e,
 #pragma unroll
     for (int j = 0; j < B; ++j) {
       const int64_t x = en + int64_t(j) * st;
-      t2[j] = x < ee ? base + __ldg(tgt + x) : u;
+      t2[j] = x < ee ? base + ld_edge(tgt + x) : u;
       w2[j] = x < ee ? edge_w<UNIT>(wt, x) : 0.0f;
     }
 #pragma unroll
@@ -99,7 +130,7 @@ __device__ __forceinline__ void rescan_range(Sketch<S> &sk, uint32_t u, int64_t 
 #pragma unroll
   for (int i = 0; i < S; ++i) sk.w[i] = 0.0f;
   for (; e < ee; ++e) {
-    const uint32_t v = base + __ldg(tgt + e);
+    const uint32_t v = base + ld_edge(tgt + e);
     if (v == u) continue;
     const uint32_t c = vin[v];
     const float w = edge_w<UNIT>(wt, e);
@@ -129,7 +160,7 @@ __device__ __forceinline__ void mark_range(uint32_t u, int64_t e, int64_t ee, in
 #pragma unroll
   for (int j = 0; j < MB; ++j) {
     const int64_t x = e + int64_t(j) * st;
-    v[j] = x < ee ? base + __ldg(tgt + x) : u;
+    v[j] = x < ee ? base + ld_edge(tgt + x) : u;
   }
   while (e < ee) {
     uint32_t f[MB];
@@ -140,7 +171,7 @@ __device__ __forceinline__ void mark_range(uint32_t u, int64_t e, int64_t ee, in
 #pragma unroll
     for (int j = 0; j < MB; ++j) {
       const int64_t x = en + int64_t(j) * st;
-      v2[j] = x < ee ? base + __ldg(tgt + x) : u;
+      v2[j] = x < ee ? base + ld_edge(tgt + x) : u;
     }
 #pragma unroll
     for (int j = 0; j < MB; ++j)
@@ -182,7 +213,7 @@ __device__ __forceinline__ void exact_group_scan(Sketch<S> &sk, uint32_t u, int6
       float w = 0.0f;
       int ok = 0;
       if (e < ee) {
-        const uint32_t v = base + __ldg(tgt + e);
+        const uint32_t v = base + ld_edge(tgt + e);
         w = edge_w<UNIT>(wt, e);
         c = vin[v];
         ok = v != u;

@@ -14,7 +14,12 @@
 // call left in it: each call clears what must start at zero, and calls that overlap on the GPU
 // (other streams, other host threads) race on it. The array's device address is looked up once
 // per device, by the first call on that device, with that device current; make that first call
-// before any stream capture.
+// before any stream capture. CUDA loads code and places __device__ arrays lazily: this file's
+// module (and with it the array) is put on a device by that first call, and each kernel variant
+// the call launches (slot count, mode, offset width, weighted or unit) by the first call that uses
+// it. Those loads are the runtime's own device allocations, so a caller that is about to hand the
+// device's memory to a pool makes one call of each variant it will use first. The caller's current
+// device is restored before returning.
 #include <cuda_runtime.h>
 
 #include <cub/device/device_scan.cuh>
@@ -87,6 +92,13 @@ inline int blocks_for(int64_t n) {
   return int(b < 1 ? 1 : (b > 148 * 32 ? 148 * 32 : b));
 }
 
+// Restores the calling thread's current device on every return path.
+struct DeviceGuard {
+  int saved = -1;
+  DeviceGuard() { if (cudaGetDevice(&saved) != cudaSuccess) { saved = -1; cudaGetLastError(); } }
+  ~DeviceGuard() { if (saved >= 0) cudaSetDevice(saved); }
+};
+
 #define NA_TRY(expr)                                                      \
   do {                                                                    \
     const cudaError_t _e = (expr);                                        \
@@ -117,10 +129,13 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   const int rescan = o->rescan < 0 ? (exact ? 1 : 0) : (o->rescan ? 1 : 0);
   if (rescan && !exact && slots > 1) return RAK_ERR_UNSUPPORTED;
   if (o->sketch_rule > 2 || o->label_order > 2) return RAK_ERR_INVALID_ARGUMENT;
-  // the reference label order needs its own n-sized tables: this entry labels by vertex id
-  if ((exact && o->sketch_rule == 2) || o->label_order == 2) return RAK_ERR_UNSUPPORTED;
+  if (exact && o->sketch_rule == 2) return RAK_ERR_UNSUPPORTED;
+  // labels as in rak_lowmem_cuda: asynchronous runs default to positions in the reference GPU
+  // path's vertex order (two n-sized tables more in the array); the synchronous modes label by id
+  const int order_kind = o->label_order <= 0 ? (sync ? 1 : 2) : o->label_order;
+  if (order_kind == 2 && sync) return RAK_ERR_UNSUPPORTED;
   const int iters = o->max_iterations;
-  if (iters < 0 || iters > 1024 || !(o->tolerance >= 0)) return RAK_ERR_INVALID_ARGUMENT;
+  if (iters < 0 || iters > 1024 || !(o->tolerance >= 0) || o->wait_timeout_ns < 0) return RAK_ERR_INVALID_ARGUMENT;
   Layout ly;
   ly.lane_max = o->lane_max > 0 ? o->lane_max : DEFAULT_LANE_MAX;
   ly.hub_min = o->hub_min > 0 ? o->hub_min : DEFAULT_HUB_MIN;
@@ -131,6 +146,7 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   std::memset(rr, 0, sizeof(*rr));
   rr->modularity = std::numeric_limits<double>::quiet_NaN();
 
+  DeviceGuard keep_device;
   NA_TRY(cudaSetDevice(device));
   unsigned char *base = nullptr;
   rak_status s = scratch_base(device, &base);
@@ -143,6 +159,9 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   Carve cv{base};
   unsigned int *bad = cv.take<unsigned int>(1);
   uint32_t *order = cv.take<uint32_t>(size_t(n > 0 ? n : 1));
+  const bool ref_labels = order_kind == 2 && n > 0;
+  uint32_t *ref_ks = ref_labels ? cv.take<uint32_t>(size_t(n)) : nullptr;
+  uint32_t *ref_pos = ref_labels ? cv.take<uint32_t>(size_t(n)) : nullptr;
   const size_t plan_mark = cv.used;
 
   // ---- plan: per-vertex keys, stable radix sort into regions, key histogram -------------------
@@ -175,6 +194,14 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
     NA_TRY(cudaStreamSynchronize(st));
   }
   cv.used = plan_mark;  // sort space is dead from here on
+  if (ref_labels) {
+    // the reference order (depends on degrees only), built in the dead sort space
+    void *ref_tmp = cv.take<unsigned char>(ref_order_scratch_bytes(n, 1));
+    if (cv.need > RAK_NOALLOC_SCRATCH_BYTES) { rr->peak_device_bytes = cv.need; return RAK_ERR_OUT_OF_MEMORY; }
+    NA_TRY(ref_order(g->offsets, off64, n, nullptr, nullptr, 0, ref_ks, ref_pos, ref_tmp, st));
+    NA_TRY(cudaStreamSynchronize(st));
+    cv.used = plan_mark;
+  }
 
   // ---- split-vertex chunk tables, built on the device --------------------------------------------
   const int64_t nhub = int64_t(h[0]);
@@ -238,8 +265,11 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   NA_TRY(cudaMemsetAsync(moved, 0xFF, size_t(nhub > 0 ? nhub : 1) * 4, st));
   NA_TRY(cudaMemsetAsync(stats, 0, size_t(it_slots) * STATS_STRIDE * 8, st));
   NA_TRY(cudaMemsetAsync(rs, 0, sizeof(RunStateHost), st));
+  // the kernel's code is loaded (CUDA loads modules lazily) before the timed part
+  if (iters > 0) NA_TRY(prepare_lpa(slots, mode, off64, g->weights == nullptr, false));
   const auto t1 = std::chrono::steady_clock::now();
-  NA_TRY(launch_init(membership, vcom1, q, n, st));
+  if (ref_labels) NA_TRY(launch_init_mapped(membership, q, ref_pos, n, st));
+  else NA_TRY(launch_init(membership, vcom1, q, n, st));
   NA_TRY(launch_init_flags(aff0, aff1, o->initial_flags, n, st));
   LpaArgs a{};
   a.off = g->offsets; a.tgt = g->targets; a.wt = g->weights; a.n = n;
@@ -255,7 +285,7 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   a.mark_test = mark_test_for(slots, n, g->m);
   // rule sets as in rak_lowmem_cuda: the CPU rules unless sketch_rule asks for the GPU ones
   a.gpu_rule = mode != RAK_MODE_SYNC && o->sketch_rule == 2;
-  a.timeout_ns = 20LL * 1000 * 1000 * 1000;
+  a.timeout_ns = o->wait_timeout_ns > 0 ? (long long)o->wait_timeout_ns : DEFAULT_WAIT_TIMEOUT_NS;
   if (iters > 0) {
     int grid = 0;
     NA_TRY(launch_lpa(a, slots, mode, off64, st, &grid));
@@ -269,6 +299,10 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   const int done = iters > 0 ? int(hs.iterations) : 0;
   if (sync && (done & 1)) {
     NA_TRY(cudaMemcpyAsync(membership, vcom1, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
+    NA_TRY(cudaStreamSynchronize(st));
+  }
+  if (ref_labels) {
+    NA_TRY(launch_labels_to_ids(membership, ref_ks, n, st));
     NA_TRY(cudaStreamSynchronize(st));
   }
   const auto t2 = std::chrono::steady_clock::now();

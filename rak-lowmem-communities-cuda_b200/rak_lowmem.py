@@ -44,7 +44,7 @@ class rak_options(C.Structure):
                 ("hub_min", C.c_int32), ("hub_chunk", C.c_int32), ("validate", C.c_int32),
                 ("compute_modularity", C.c_int32), ("start_iteration", C.c_int32),
                 ("initial_flags", C.c_void_p), ("sketch_rule", C.c_int32), ("label_order", C.c_int32),
-                ("reserved", C.c_int64 * 7)]
+                ("wait_timeout_ns", C.c_int64), ("reserved", C.c_int64 * 6)]
 
 
 class rak_result(C.Structure):

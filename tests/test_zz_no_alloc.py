@@ -7,7 +7,8 @@ Checked through the C ABI against the allocating entry point rak_lowmem_cuda on 
 device-located graphs, twice in a row (the array keeps the previous call's contents, so the second
 call shows that everything that must start from zero is cleared). The synchronous modes are
 deterministic, so the labels must be identical; the split mode exercises the split-vertex partial
-sketches and arrival counters that live in the array.
+sketches and arrival counters that live in the array. The default asynchronous mode is checked for
+valid labels and modularity, and a repeated call for unchanged free device memory.
 """
 import numpy as np
 import pytest
@@ -70,14 +71,51 @@ def test_noalloc_refuses_graphs_beyond_the_array():
     assert "bytes of scratch" in str(e.value)
 
 
-def test_noalloc_labels_by_id_only():
+def test_noalloc_async_default_is_valid_and_matches_quality():
+    """The default asynchronous mode (reference label order, in-place updates) is not deterministic:
+    its labels must be valid vertex ids and its modularity close to the allocating entry point's."""
+    import torch
+    g = rl.gen_sbm(20000, 40, 12.0, 20.0, seed=26)
+    keep, csr = device_graph(g)
+    with rl.Context(0) as ctx:
+        want = torch.empty(g.n, dtype=torch.int32, device="cuda")
+        ref = ctx.lowmem_device(csr, want, compute_modularity=1)
+    for call in range(2):
+        got = torch.full((g.n,), -1, dtype=torch.int32, device="cuda")
+        res = rl.lowmem_noalloc(0, None, csr, got, compute_modularity=1)
+        torch.cuda.synchronize()
+        lab = got.cpu().numpy()
+        assert lab.min() >= 0 and lab.max() < g.n, f"call {call}: labels outside the vertex ids"
+        assert res.iterations >= 1
+        assert res.modularity == pytest.approx(ref.modularity, rel=0.02), (call, res.modularity, ref.modularity)
+
+
+def test_noalloc_label_orders():
     import torch
     g = rl.gen_rmat(10, 8, seed=25)
     keep, csr = device_graph(g)
     out = torch.empty(g.n, dtype=torch.int32, device="cuda")
-    with pytest.raises(rl.RakError) as e:
-        rl.lowmem_noalloc(0, None, csr, out, label_order=2)
+    with pytest.raises(rl.RakError) as e:        # synchronous modes label by id, as rak_lowmem_cuda
+        rl.lowmem_noalloc(0, None, csr, out, mode=rl.MODE_SYNC, label_order=2)
     assert e.value.status == 7
-    res = rl.lowmem_noalloc(0, None, csr, out, label_order=1, sketch_rule=2)
+    for order in (1, 2):
+        res = rl.lowmem_noalloc(0, None, csr, out, label_order=order, sketch_rule=2)
+        torch.cuda.synchronize()
+        assert res.iterations >= 1 and 0 <= int(out.min()) and int(out.max()) < g.n
+
+
+def test_noalloc_second_call_takes_no_device_memory():
+    """After a first call of a variant (which may load that variant's code onto the device), a
+    second identical call leaves the device's free memory unchanged."""
+    import torch
+    g = rl.gen_rmat(12, 8, seed=27, w_lo=1.0, w_hi=10.0)
+    keep, csr = device_graph(g)
+    out = torch.empty(g.n, dtype=torch.int32, device="cuda")
+    opts = dict(mode=rl.MODE_SYNC_SPLIT, slots=8, compute_modularity=1, **SPLIT_LAYOUT)
+    rl.lowmem_noalloc(0, None, csr, out, **opts)
     torch.cuda.synchronize()
-    assert res.iterations >= 1 and int(out.max()) < g.n
+    free0, _ = torch.cuda.mem_get_info(0)
+    rl.lowmem_noalloc(0, None, csr, out, **opts)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0, (free0, free1)
