@@ -110,7 +110,15 @@ typedef struct rak_options {
                                  status with the context still usable (the reference has no bound:
                                  a stuck kernel hangs its blocking read-back, inc/rakLowmemCuda.hxx
                                  :486, and errors exit(), inc/_cuda.hxx:221-235) */
-  int64_t reserved[6];
+  int32_t tie_break;          /* -1 or 0: mode default; 1: the reference's tie rule for Misra-Gries
+                                 sketches (inc/rakLowmem.hxx:164-171: the first slot of maximum
+                                 weight, which is the most recently inserted key); 2: on iterations
+                                 l < tie_iterations a maximum shared by several slots goes to the
+                                 key with the largest hash of (vertex, key, l) (SplitMix64), then
+                                 the reference's rule. CPU sketch rules only. ASYNC: 2 [2]; SYNC
+                                 and SYNC_SPLIT: 1 [1], 2 on request (deterministic) */
+  int32_t tie_iterations;     /* 0: default [4]; iterations with hashed ties under tie_break 2 */
+  int64_t reserved[5];
 } rak_options;
 
 typedef struct rak_result {

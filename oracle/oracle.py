@@ -51,7 +51,7 @@ class orc_layout(C.Structure):
 class orc_opts(C.Structure):
     _fields_ = [("slots", C.c_int), ("rescan", C.c_int), ("split", C.c_int), ("layout", orc_layout),
                 ("tolerance", C.c_double), ("max_iterations", C.c_int), ("pickless_step", C.c_int),
-                ("check_on_pickless", C.c_int), ("gpu_rule", C.c_int)]
+                ("check_on_pickless", C.c_int), ("gpu_rule", C.c_int), ("tie_until", C.c_int)]
 
 
 class orc_sketch(C.Structure):
@@ -71,6 +71,9 @@ _sig(_o, "orc_mg_accumulate", None, C.POINTER(orc_sketch), C.c_int, C.c_uint32, 
 _sig(_o, "orc_bm_accumulate", None, C.POINTER(orc_sketch), C.c_uint32, C.c_float)
 _sig(_o, "orc_sketch_merge", None, C.POINTER(orc_sketch), C.POINTER(orc_sketch), C.c_int)
 _sig(_o, "orc_sketch_choose", None, C.POINTER(orc_sketch), C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_float))
+_sig(_o, "orc_tie_hash", C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32)
+_sig(_o, "orc_sketch_choose_hashed", None, C.POINTER(orc_sketch), C.c_int, C.c_uint32, C.c_uint32,
+     C.POINTER(C.c_uint32), C.POINTER(C.c_float))
 _sig(_o, "orc_mg_accumulate_gpu", None, C.POINTER(orc_sketch), C.c_int, C.c_uint32, C.c_float)
 _sig(_o, "orc_sketch_choose_gpu", None, C.POINTER(orc_sketch), C.c_int, C.POINTER(C.c_uint32), C.POINTER(C.c_float))
 _sig(_o, "orc_choose", None, C.POINTER(orc_csr), C.POINTER(orc_opts), C.c_uint32, P, C.POINTER(C.c_uint32),
@@ -103,9 +106,9 @@ class Graph:
 
 
 def make_opts(slots=8, rescan=0, split=0, layout=DEFAULT_LAYOUT, tolerance=0.05, max_iterations=20,
-              pickless_step=0, check_on_pickless=1, gpu_rule=0) -> orc_opts:
+              pickless_step=0, check_on_pickless=1, gpu_rule=0, tie_until=0) -> orc_opts:
     return orc_opts(slots, rescan, split, orc_layout(*layout), tolerance, max_iterations, pickless_step,
-                    check_on_pickless, gpu_rule)
+                    check_on_pickless, gpu_rule, tie_until)
 
 
 def sync_step(g, o: orc_opts, iteration, vcom_prev, aff_prev):

@@ -96,6 +96,28 @@ void orc_sketch_choose(const orc_sketch *s, int slots, uint32_t *c, float *w) {
   *c = cm; *w = wm;
 }
 
+static uint64_t mix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+uint64_t orc_tie_hash(uint32_t u, uint32_t key, uint32_t l) {
+  return mix64((((uint64_t)key << 32) | (uint64_t)u) ^ ((uint64_t)l * 0xD6E8FEB86659FD93ull));
+}
+
+void orc_sketch_choose_hashed(const orc_sketch *s, int slots, uint32_t u, uint32_t l, uint32_t *c, float *w) {
+  uint32_t cm = ORC_NONE;
+  float wm = 0.0f;
+  uint64_t hb = 0;
+  for (int i = 0; i < slots; ++i) {
+    const uint64_t h = orc_tie_hash(u, s->k[i], l);
+    if (s->w[i] > wm || (s->w[i] == wm && wm > 0.0f && h > hb)) { wm = s->w[i]; cm = s->k[i]; hb = h; }
+  }
+  *c = cm; *w = wm;
+}
+
 /* Sequential scan of edges [b, e) of u with stride st (self-loops skipped, rakLowmem.hxx:65). */
 static void scan_range(const orc_csr *g, uint32_t u, const uint32_t *vcom, int slots,
                        int64_t b, int64_t e, int64_t st, orc_sketch *s, int gpu) {
@@ -181,8 +203,9 @@ static void rescan(const orc_csr *g, uint32_t u, const uint32_t *vcom, int slots
   }
 }
 
-void orc_choose(const orc_csr *g, const orc_opts *o, uint32_t u, const uint32_t *vcom,
-                uint32_t *c, float *w) {
+/* The per-vertex choice on iteration l (l < 0: outside any iteration, no hashed ties). */
+static void choose_at(const orc_csr *g, const orc_opts *o, uint32_t u, const uint32_t *vcom, int l,
+                      uint32_t *c, float *w) {
   orc_sketch s;
   if (o->split) {
     split_sketch(g, o, u, vcom, &s);
@@ -192,7 +215,13 @@ void orc_choose(const orc_csr *g, const orc_opts *o, uint32_t u, const uint32_t 
     if (o->rescan && o->slots > 1) rescan(g, u, vcom, o->slots, &s);
   }
   if (o->gpu_rule) orc_sketch_choose_gpu(&s, o->slots, c, w);
+  else if (o->slots > 1 && l >= 0 && l < o->tie_until) orc_sketch_choose_hashed(&s, o->slots, u, (uint32_t)l, c, w);
   else orc_sketch_choose(&s, o->slots, c, w);
+}
+
+void orc_choose(const orc_csr *g, const orc_opts *o, uint32_t u, const uint32_t *vcom,
+                uint32_t *c, float *w) {
+  choose_at(g, o, u, vcom, -1, c, w);
 }
 
 static int is_pickless(const orc_opts *o, int l) { return o->pickless_step > 0 && l % o->pickless_step == 0; }
@@ -216,7 +245,7 @@ uint64_t orc_sync_step(const orc_csr *g, const orc_opts *o, int iteration,
     if (deg == 0) continue;
     ++processed; edges += (uint64_t)deg;
     uint32_t d = vcom_prev[u], c; float w;
-    orc_choose(g, o, (uint32_t)u, vcom_prev, &c, &w);
+    choose_at(g, o, (uint32_t)u, vcom_prev, iteration, &c, &w);
     /* CPU rule: w > 0; GPU rule: w != 0 for Misra-Gries, any candidate for Boyer-Moore */
     const int weight_ok = o->gpu_rule ? (o->slots == 1 || w != 0.0f) : (w > 0.0f);
     if (!weight_ok || c == d) continue;

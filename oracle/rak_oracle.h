@@ -58,6 +58,9 @@ typedef struct orc_opts {
   int gpu_rule;           /* 0: the reference CPU sketch rules; 1: its GPU rules (first free slot,
                              no clamp, tournament argmax, move if w != 0, Boyer-Moore from the
                              vertex's own label) */
+  int tie_until;          /* CPU rules, Misra-Gries: on iterations l < tie_until a maximum shared by
+                             several slots goes to the key with the largest orc_tie_hash(u, key, l);
+                             0: the reference's linear first maximum throughout */
 } orc_opts;
 
 typedef struct orc_sketch {
@@ -73,6 +76,13 @@ void orc_sketch_merge(orc_sketch *a, const orc_sketch *b, int slots);
 void orc_sketch_choose(const orc_sketch *s, int slots, uint32_t *c, float *w);
 void orc_mg_accumulate_gpu(orc_sketch *s, int slots, uint32_t c, float w);
 void orc_sketch_choose_gpu(const orc_sketch *s, int slots, uint32_t *c, float *w);
+
+/* SplitMix64 finaliser (Steele, Lea & Flood, OOPSLA 2014) of (key << 32 | u) ^ l * 0xD6E8FEB86659FD93:
+ * the tie order of the library's hashed ties (rak_options.tie_break 2). */
+uint64_t orc_tie_hash(uint32_t u, uint32_t key, uint32_t l);
+/* Largest weight; among equal maximum weights the key with the largest orc_tie_hash (lower slot on
+ * equal hashes). */
+void orc_sketch_choose_hashed(const orc_sketch *s, int slots, uint32_t u, uint32_t l, uint32_t *c, float *w);
 
 /* Best label of vertex u given a label snapshot vcom (before the move rule is applied). */
 void orc_choose(const orc_csr *g, const orc_opts *o, uint32_t u, const uint32_t *vcom,

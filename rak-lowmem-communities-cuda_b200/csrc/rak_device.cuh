@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "rak_hash.hpp"
+
 namespace rak {
 
 constexpr uint32_t NONE = 0xFFFFFFFFu;  // sketch key that matches no community
@@ -149,6 +151,26 @@ __device__ __forceinline__ void sk_choose(const Sketch<S> &s, uint32_t &c, float
 #pragma unroll
     for (int i = 0; i < S; ++i)
       if (s.w[i] > w) { w = s.w[i]; c = s.k[i]; }
+  }
+}
+
+// Tie rule of hashed ties: the CPU rules' argmax (largest weight) except that a maximum shared by
+// several slots goes to the key with the largest tie_hash(u, key, l) -- a fixed pseudo-random order
+// per vertex and iteration, so no neighbour position is preferred the way "most recently inserted"
+// prefers the last neighbour in edge order (on grids: one direction). Ties between equal hashes keep
+// the lower slot.
+__host__ __device__ __forceinline__ uint64_t tie_hash(uint32_t u, uint32_t key, uint32_t l) {
+  return mix64((uint64_t(key) << 32 | uint64_t(u)) ^ (uint64_t(l) * 0xD6E8FEB86659FD93ull));
+}
+template <int S>
+__device__ __forceinline__ void sk_choose_hashed(const Sketch<S> &s, uint32_t u, uint32_t l, uint32_t &c, float &w) {
+  c = NONE;
+  w = 0.0f;
+  uint64_t hb = 0;
+#pragma unroll
+  for (int i = 0; i < S; ++i) {
+    const uint64_t h = tie_hash(u, s.k[i], l);
+    if (s.w[i] > w || (s.w[i] == w && w > 0.0f && h > hb)) { w = s.w[i]; c = s.k[i]; hb = h; }
   }
 }
 

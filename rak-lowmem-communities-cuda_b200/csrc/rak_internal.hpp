@@ -57,6 +57,8 @@ constexpr int64_t DEFAULT_LANE_MAX = 256;
 constexpr int64_t DEFAULT_HUB_MIN = 65536;
 constexpr int64_t DEFAULT_HUB_CHUNK = 8192;
 constexpr int64_t MAX_LANE_MAX = 1024;
+// Iterations with hashed ties (rak_options.tie_break 2) when rak_options.tie_iterations is 0.
+constexpr int DEFAULT_TIE_ITERATIONS = 4;
 // Bound on each device-side wait when rak_options.wait_timeout_ns is 0.
 constexpr long long DEFAULT_WAIT_TIMEOUT_NS = 20LL * 1000 * 1000 * 1000;
 
@@ -111,6 +113,7 @@ struct LpaArgs {
   int grid_cap;                 // at most this many blocks (0: as many as fit), to share the GPU
   int mark_test;                // neighbour marking reads a flag before storing it (mark_test_for)
   int gpu_rule;                 // synchronous split mode: the reference GPU sketch rules (else CPU)
+  int tie_until;                // iterations l < tie_until break Misra-Gries ties by hash (CPU rules)
   int iters;
   int start_iter;
   double tolerance;

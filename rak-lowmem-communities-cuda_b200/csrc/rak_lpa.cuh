@@ -45,12 +45,12 @@ struct G_ {
   const float *wt;
 };
 
-// Edge-stream loads (targets, weights). An iteration reads each of them once, so they carry an L2
-// evict-first cache policy (an operand of the load instruction, not a setting of the GPU): the L2's
-// capacity stays with the neighbour-label gathers, which repeat (a label is read once per incident
-// edge). RAK_STREAM_HINT=0 compiles plain non-coherent loads instead.
+// Edge-stream loads (targets, weights): non-coherent loads. RAK_STREAM_HINT=1 gives them an L2
+// evict-first cache policy (an operand of the load instruction, not a setting of the GPU), meant to
+// leave L2 capacity to the label gathers; measured on B200 it was 2-3% slower (R-MAT scale 27: 116
+// vs 119 G edges/s; scale 24 weighted: 126 vs 128), so it is off.
 #ifndef RAK_STREAM_HINT
-#define RAK_STREAM_HINT 1
+#define RAK_STREAM_HINT 0
 #endif
 __device__ __forceinline__ uint64_t l2_stream_policy() {
   uint64_t p;
@@ -194,6 +194,180 @@ __device__ __forceinline__ void mark_item(const LpaArgs &a, uint32_t u, int64_t 
   }
 }
 
+// ---- edge tiles staged in shared memory by the bulk-copy engine (TMA) -------------------------
+//
+// Lane groups (G lanes per vertex, regions 1-5) and split-vertex chunks (region 0, G = 32) scan
+// contiguous edge ranges. Instead of every lane loading its targets and weights from global memory
+// a few edges ahead, each group's range is copied tile by tile into shared memory with 1-D bulk
+// copies (cp.async.bulk, completion counted in bytes on an mbarrier), STG_STAGES tiles ahead of the
+// lanes, and the lanes read their edges there. Lane s of a group still accumulates edges eb+s,
+// eb+s+G, ... in that order, so sketches are bit-identical to scan_range's. Bulk copies need
+// 16-byte aligned addresses and sizes: the few edges before the first aligned address of a range
+// and after its last one are read from global memory directly, so no copy reads outside [eb, ee).
+// The source is always this GPU's own memory; no copy uses a multicast form.
+#ifndef RAK_STAGE
+#define RAK_STAGE 1
+#endif
+constexpr int LPA_WARPS = 8;      // warps per block (256 threads)
+constexpr int STG_TILE = 256;     // edges per warp per stage, divided among the warp's lane groups
+constexpr int STG_BUF = STG_TILE + 64;  // per stage: group slices padded by 4 edges (bank spread)
+constexpr int STG_STAGES = 3;     // tiles in flight per warp
+constexpr int STG_B = 4;          // edges per lane per gather batch from a staged tile
+
+// Dynamic shared memory of an lpa_run block that stages tiles: per warp STG_STAGES buffers of
+// targets (and of weights, for weighted graphs), then one mbarrier per buffer.
+__host__ __device__ constexpr size_t stage_bytes(bool unit) {
+  return size_t(LPA_WARPS) * STG_STAGES * STG_BUF * 4 * (unit ? 1 : 2) + size_t(LPA_WARPS) * STG_STAGES * 8;
+}
+
+struct StageCtx {
+  uint32_t *t;     // this warp's target buffers (STG_STAGES x STG_BUF)
+  float *w;        // this warp's weight buffers (weighted graphs)
+  uint32_t bar;    // shared-memory address of this warp's first mbarrier
+  uint32_t phase;  // per buffer, the parity of the next completion to wait for (warp-uniform)
+  bool on;         // staging in use for this launch
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_arrive(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// 1-D bulk copy global -> this CTA's shared memory, completing `bytes` on the mbarrier; the edge
+// stream keeps its L2 evict-first policy.
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+#if RAK_STREAM_HINT
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
+      ::"r"(dst), "l"(src), "r"(bytes), "r"(bar), "l"(l2_stream_policy())
+      : "memory");
+#else
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+#endif
+}
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// Waits for the completion of `parity` on an mbarrier, for at most timeout_ns of wall time. On
+// expiry it records RAK_ERR_TIMEOUT and the launch's abort flag, as the grid barrier does (the
+// launch then ends at its next barrier), and returns false: the caller reads that tile's edges
+// from global memory instead.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, RunState *rs, long long timeout_ns) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try(bar, parity)) {
+    if ((long long)(global_ns() - t0) > timeout_ns) {
+      atomicCAS(&rs->error, 0u, 5u);
+      atomicExch(&rs->abort, 1u);
+      return false;
+    }
+  }
+  return true;
+}
+
+// Issues tile k of a group's copy range [cs, ce) (tiles of `slice` edges) into buffer k % STG_STAGES.
+// Called by every lane of the warp; lane 0 arms the buffer's mbarrier with the bytes of all
+// groups' copies, then each group's first lane starts its copies.
+template <bool UNIT>
+__device__ __forceinline__ void stage_issue(const StageCtx &sc, int k, int64_t cs, int64_t ce, int slice, int off,
+                                            bool leader, const uint32_t *tgt, const float *wt) {
+  const int buf = k % STG_STAGES;
+  const int64_t tb = cs + int64_t(k) * slice;
+  const int64_t te = tb + slice < ce ? tb + slice : ce;
+  const uint32_t bytes = te > tb ? uint32_t(te - tb) * 4u : 0u;
+  const uint32_t total = __reduce_add_sync(FULL, leader ? bytes : 0u) * (UNIT ? 1u : 2u);
+  const uint32_t bar = sc.bar + 8u * uint32_t(buf);
+  fence_proxy_async_smem();  // this buffer's earlier reads come before the copy that refills it
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) mbar_expect_arrive(bar, total);
+  __syncwarp();
+  if (leader && bytes) {
+    bulk_g2s(smem_u32(sc.t + buf * STG_BUF + off), tgt + tb, bytes, bar);
+    if constexpr (!UNIT) bulk_g2s(smem_u32(sc.w + buf * STG_BUF + off), wt + tb, bytes, bar);
+  }
+}
+
+// Staged form of scan_range for the lane groups of a warp: lane s of the group of G lanes that
+// owns u accumulates edges eb+s, eb+s+G, ... < ee in that order. Every lane of the warp calls it
+// (the tile loop is warp-uniform); a group with nothing to scan passes eb == ee.
+template <int S, bool UNIT, int RULE>
+__device__ __forceinline__ void staged_scan(Sketch<S> &sk, StageCtx &sc, uint32_t u, int64_t eb, int64_t ee, int G,
+                                            int s, const uint32_t *tgt, const float *wt, const uint32_t *vin,
+                                            uint32_t base, RunState *rs, long long timeout_ns) {
+  const int lane = threadIdx.x & 31;
+  const int slice = STG_TILE / 32 * G;                                // edges per group per tile
+  const int off = (lane / G) * (slice + (G < 32 ? 4 : 0));            // the group's part of a buffer
+  // Copies cover [cs, ce): cs the first edge at a 16-byte aligned address at or after eb, ce the
+  // last such boundary at or before ee. Tile k copies [cs + k*slice, min(cs + (k+1)*slice, ce));
+  // the lanes take edges before cs in tile 0 and after ce in the group's last tile from global.
+  int64_t cs = eb + int64_t(((16u - (uint32_t(reinterpret_cast<uintptr_t>(tgt + eb)) & 15u)) & 15u) >> 2);
+  if (cs > ee) cs = ee;
+  const int64_t ce = cs + ((ee - cs) & ~int64_t(3));
+  int nt = ee > eb ? int((ee - cs + slice - 1) / slice) : 0;
+  if (ee > eb && nt < 1) nt = 1;
+  const int ntiles = int(__reduce_max_sync(FULL, unsigned(nt)));
+  const bool leader = s == 0;
+  for (int k = 0; k < STG_STAGES && k < ntiles; ++k)
+    stage_issue<UNIT>(sc, k, cs, k < nt ? ce : cs, slice, off, leader, tgt, wt);
+  int rel = int(eb - cs) + s;   // the lane's next edge, relative to the current tile's first edge
+  for (int k = 0; k < ntiles; ++k) {
+    const int buf = k % STG_STAGES;
+    const bool ok = mbar_wait(sc.bar + 8u * uint32_t(buf), (sc.phase >> buf) & 1u, rs, timeout_ns);
+    sc.phase ^= 1u << buf;
+    const int64_t tb = cs + int64_t(k) * slice;
+    // relative bounds: the tile's edges end at hi (the group's last tile takes the tail), the
+    // copied ones at se
+    const int hi = k + 1 >= nt ? int(ee - tb) : (slice < ee - tb ? slice : int(ee - tb));
+    const int se = ok ? (slice < ce - tb ? slice : int(ce - tb)) : 0;
+    const uint32_t *bt = sc.t + buf * STG_BUF + off;
+    const float *bw = sc.w + buf * STG_BUF + off;
+    while (rel < hi) {
+      const int left = (hi - rel + G - 1) / G;
+      const int take = left < STG_B ? left : STG_B;
+      uint32_t t[STG_B];
+      float w[STG_B];
+#pragma unroll
+      for (int j = 0; j < STG_B; ++j) {
+        const int x = rel + j * G;
+        t[j] = u;
+        w[j] = 0.0f;
+        if (j < take) {
+          const bool in = x >= 0 && x < se;
+          t[j] = base + (in ? bt[x] : ld_edge(tgt + (tb + x)));
+          if constexpr (UNIT) w[j] = 1.0f;
+          else w[j] = in ? bw[x] : ld_weight(wt + (tb + x));
+        }
+      }
+      uint32_t c[STG_B];
+#pragma unroll
+      for (int j = 0; j < STG_B; ++j) c[j] = vin[t[j]];
+#pragma unroll
+      for (int j = 0; j < STG_B; ++j)
+        if (t[j] != u) sk_acc<S, RULE>(sk, c[j], w[j]);
+      rel += take * G;
+    }
+    rel -= slice;
+    __syncwarp();
+    if (k + STG_STAGES < ntiles)
+      stage_issue<UNIT>(sc, k + STG_STAGES, cs, k + STG_STAGES < nt ? ce : cs, slice, off, leader, tgt, wt);
+  }
+}
+
 // Exact edge-order scan of u by the G lanes of one aligned group: lanes load G edges at a time,
 // then every lane applies them in order from shuffles, so all lanes hold the same sketch as a
 // single sequential scan would build (and, with rescan, the same exact weights).
@@ -265,6 +439,22 @@ __device__ __forceinline__ bool move_rule(float w, uint32_t c, uint32_t d, bool 
   return weight_ok && c != d && !(pickless && c > d);
 }
 
+// Argmax of a vertex's sketch under the launch's tie rule: hashed ties on iterations
+// l < a.tie_until (Misra-Gries, CPU rules), else the rule set's own. u_local: the vertex's id within
+// its graph, so a graph breaks its ties the same way alone and in a batch.
+template <int S, int RULE>
+__device__ __forceinline__ void choose(const LpaArgs &a, const Sketch<S> &sk, uint32_t u_local, int it, uint32_t &c,
+                                       float &w) {
+  if constexpr (S > 1 && RULE == RULE_CPU) {
+    const int l = a.start_iter + it;
+    if (l < a.tie_until) {
+      sk_choose_hashed<S>(sk, u_local, uint32_t(l), c, w);
+      return;
+    }
+  }
+  sk_choose<S, RULE>(sk, c, w);
+}
+
 // Region 6: one lane per vertex. Items are collected into a per-warp queue of active vertices
 // (inactive ones are settled at once), and the queue is processed 32 vertices at a time so every
 // lane has work; region 6 is sorted by degree, so a batch holds vertices of similar degree.
@@ -306,7 +496,7 @@ __device__ __forceinline__ void lane_batch(const LpaArgs &a, const G_<O> &g, con
     if (a.rescan) rescan_range<S, UNIT>(sk, u, eb, ee, g.tgt, g.wt, vin, base);
   uint32_t c;
   float w;
-  sk_choose<S, RULE>(sk, c, w);
+  choose<S, RULE>(a, sk, u - base, it, c, w);
   const bool moved = move_rule<S, RULE>(w, c, d, pickless);
   cnt.processed += 1;
   cnt.edges += (unsigned long long)(ee - eb);
@@ -328,7 +518,7 @@ __device__ __forceinline__ void lane_batch(const LpaArgs &a, const G_<O> &g, con
 template <int S, int MODE, class O, bool UNIT, bool BATCH, int RULE>
 __device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, const G_<O> &g, int r, int64_t local,
                                            int it, bool pickless, const uint32_t *vin, uint32_t *vout,
-                                           uint8_t *fin, uint8_t *fout, Counters &cnt) {
+                                           uint8_t *fin, uint8_t *fout, Counters &cnt, StageCtx &sc) {
   const int G = region_group(r);
   const int lane = threadIdx.x & 31, grp = lane / G, s = lane & (G - 1);
   const int64_t idx = local * (32 / G) + grp;
@@ -347,12 +537,16 @@ __device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, 
   if constexpr (MODE == MODE_SYNC) {
     if (active) exact_group_scan<S, UNIT>(sk, u, eb, ee, G, grp, s, S > 1 && a.rescan, g.tgt, g.wt, vin, base);
   } else {
-    if (active) scan_range<S, UNIT, RULE>(sk, u, eb + s, ee, G, g.tgt, g.wt, vin, base);
+    if (sc.on)
+      staged_scan<S, UNIT, RULE>(sk, sc, u, active ? eb : 0, active ? ee : 0, G, s, g.tgt, g.wt, vin, base,
+                                 static_cast<RunState *>(a.rs), a.timeout_ns);
+    else if (active)
+      scan_range<S, UNIT, RULE>(sk, u, eb + s, ee, G, g.tgt, g.wt, vin, base);
     sk_tree<S, RULE>(sk, G);
   }
   uint32_t c;
   float w;
-  sk_choose<S, RULE>(sk, c, w);
+  choose<S, RULE>(a, sk, u - base, it, c, w);
   bool moved = active && move_rule<S, RULE>(w, c, d, pickless);
   moved = __shfl_sync(FULL, moved, grp * G);
   if (s == 0 && valid) {
@@ -376,7 +570,7 @@ __device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, 
 template <int S, int MODE, class O, bool UNIT, bool BATCH, int RULE>
 __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, const G_<O> &g, int64_t local, int it, bool pickless,
                                          const uint32_t *vin, uint32_t *vout, uint8_t *fin, uint8_t *fout,
-                                         Counters &cnt) {
+                                         Counters &cnt, StageCtx &sc) {
   const int lane = threadIdx.x & 31;
   const uint32_t h = __ldg(a.chunk_hub + local);
   const int64_t first = __ldg(a.hub_first + h), nch = __ldg(a.hub_first + h + 1) - first, j = local - first;
@@ -393,7 +587,7 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
     if (active) exact_group_scan<S, UNIT>(sk, u, eb, ee, 32, 0, lane, S > 1 && a.rescan, g.tgt, g.wt, vin, base);
     uint32_t c;
     float w;
-    sk_choose<S, RULE>(sk, c, w);
+    choose<S, RULE>(a, sk, u - base, it, c, w);
     const bool moved = active && move_rule<S, RULE>(w, c, d, pickless);
     if (lane == 0) {
       vout[u] = moved ? c : d;
@@ -434,7 +628,11 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
     Sketch<S> sk;
     sk_clear<S, RULE>(sk, d0);
     const int64_t cb = eb + j * a.hub_chunk, ce = cb + a.hub_chunk < ee ? cb + a.hub_chunk : ee;
-    if (active) scan_range<S, UNIT, RULE>(sk, u, cb + lane, ce, 32, g.tgt, g.wt, vin, base);
+    if (sc.on)   // active is the same on every lane
+      staged_scan<S, UNIT, RULE>(sk, sc, u, active ? cb : 0, active ? ce : 0, 32, lane, g.tgt, g.wt, vin, base,
+                                 static_cast<RunState *>(a.rs), a.timeout_ns);
+    else if (active)
+      scan_range<S, UNIT, RULE>(sk, u, cb + lane, ce, 32, g.tgt, g.wt, vin, base);
     sk_tree<S, RULE>(sk, 32);
     unsigned int last = 0;
     if (lane == 0) {
@@ -474,7 +672,7 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
     if (lane == 0) {
       uint32_t c;
       float w;
-      sk_choose<S, RULE>(acc, c, w);
+      choose<S, RULE>(a, acc, u - base, it, c, w);
       const bool moved = move_rule<S, RULE>(w, c, d, pickless);
       cnt.processed += 1;
       if constexpr (MODE == MODE_ASYNC) {
@@ -516,6 +714,22 @@ __global__ void __launch_bounds__(256, RAK_MIN_BLOCKS) lpa_run(const LpaArgs a) 
   __shared__ Regions rg;  // copied once: indexed by region at run time
   __shared__ uint32_t lq[8][64];  // per-warp queue of active one-lane vertices
   if (threadIdx.x == 0) rg = a.rg;
+  // staged edge tiles (not in the exact synchronous mode, which shuffles edges in order instead)
+  StageCtx sc{};
+  if constexpr (MODE != MODE_SYNC && RAK_STAGE) {
+    extern __shared__ __align__(128) unsigned char lpa_dsm[];
+    const int w = threadIdx.x >> 5;
+    constexpr size_t tbytes = size_t(LPA_WARPS) * STG_STAGES * STG_BUF * 4;
+    sc.t = reinterpret_cast<uint32_t *>(lpa_dsm) + size_t(w) * STG_STAGES * STG_BUF;
+    sc.w = UNIT ? nullptr : reinterpret_cast<float *>(lpa_dsm + tbytes) + size_t(w) * STG_STAGES * STG_BUF;
+    sc.bar = smem_u32(lpa_dsm + tbytes * (UNIT ? 1 : 2)) + 8u * uint32_t(w * STG_STAGES);
+    sc.phase = 0;
+    // targets and weights must share their 16-byte alignment (one copy range serves both)
+    sc.on = UNIT || ((reinterpret_cast<uintptr_t>(a.tgt) ^ reinterpret_cast<uintptr_t>(a.wt)) & 15u) == 0;
+    if (lane < STG_STAGES) mbar_init(sc.bar + 8u * uint32_t(lane), 1);
+    fence_mbar_init();
+    __syncwarp();
+  }
   unsigned int epoch = 0;
   for (int it = 0; it < a.iters; ++it) {
     if (threadIdx.x < 4) blk[threadIdx.x] = 0;
@@ -554,9 +768,9 @@ __global__ void __launch_bounds__(256, RAK_MIN_BLOCKS) lpa_run(const LpaArgs a) 
           }
         }
       } else if (r == REG_HUB) {
-        RAK_BY_RULE(hub_item, (a, rg, g, local, it, pickless, vin, vout, fin, fout, cnt));
+        RAK_BY_RULE(hub_item, (a, rg, g, local, it, pickless, vin, vout, fin, fout, cnt, sc));
       } else {
-        RAK_BY_RULE(group_item, (a, rg, g, r, local, it, pickless, vin, vout, fin, fout, cnt));
+        RAK_BY_RULE(group_item, (a, rg, g, r, local, it, pickless, vin, vout, fin, fout, cnt, sc));
       }
     }
     if (qn > 0) RAK_BY_RULE(lane_batch, (a, g, q, qn, it, pickless, vin, vout, fin, fout, cnt));
@@ -646,6 +860,9 @@ __global__ void __launch_bounds__(256, RAK_MIN_BLOCKS) lpa_run(const LpaArgs a) 
   }
 }
 
+// Dynamic shared memory of an lpa_run launch: the staged edge tiles of the modes that use them.
+inline size_t lpa_dynamic_smem(int mode, bool unit) { return (mode != MODE_SYNC && RAK_STAGE) ? stage_bytes(unit) : 0; }
+
 // The kernel instantiation for a launch and its resident blocks per SM, cached per (function,
 // device). The first query of an instantiation loads its module (CUDA loads modules lazily, which
 // can take a millisecond), so runs resolve before their timed region (prepare_lpa).
@@ -678,7 +895,10 @@ cudaError_t resolve_lpa_slots(int mode, bool off64, bool unit, bool batch, const
     }
   }
   int per_sm = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0)) != cudaSuccess) return e;
+  const size_t dyn = lpa_dynamic_smem(mode, unit);
+  if (dyn > 0 && (e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn))) != cudaSuccess)
+    return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, dyn)) != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   std::lock_guard<std::mutex> lk(mu);
   cache[{fn, dev}] = per_sm;
@@ -707,6 +927,7 @@ cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, bool batch,
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(unsigned(grid));
   cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = lpa_dynamic_smem(mode, a.wt == nullptr);
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;

@@ -44,7 +44,8 @@ class rak_options(C.Structure):
                 ("hub_min", C.c_int32), ("hub_chunk", C.c_int32), ("validate", C.c_int32),
                 ("compute_modularity", C.c_int32), ("start_iteration", C.c_int32),
                 ("initial_flags", C.c_void_p), ("sketch_rule", C.c_int32), ("label_order", C.c_int32),
-                ("wait_timeout_ns", C.c_int64), ("reserved", C.c_int64 * 6)]
+                ("wait_timeout_ns", C.c_int64), ("tie_break", C.c_int32), ("tie_iterations", C.c_int32),
+                ("reserved", C.c_int64 * 5)]
 
 
 class rak_result(C.Structure):
