@@ -310,6 +310,32 @@ def batch_mix(count, seed, threads, keep=None):
     return graphs
 
 
+def batch_mix_device(ctx, count, seed, keep=None):
+    """The batched-launch mix of batch_mix built on the device (rak_gen_rmat_device /
+    rak_gen_sbm_device: bit-identical to the host generators, seconds instead of minutes for 4096
+    graphs) and packed into one device batch. Returns (DeviceBatch, planted labels per graph or None)."""
+    import rak_lowmem as rl
+    rng = np.random.default_rng(seed)
+    dev, truths = [], []
+    for i in range(count):
+        if i % 2 == 0:
+            scale = int(rng.integers(10, 19))
+            ef = float(rng.integers(8, 33))
+            if keep is None or keep(i):
+                dev.append(rl.gen_rmat_device(ctx, scale, ef, seed=seed * 100003 + i, offset_bits=64))
+                truths.append(None)
+        else:
+            n = int(round(2.0 ** rng.uniform(10, 18)))
+            k = min(int(rng.integers(8, 1025)), n)
+            if keep is None or keep(i):
+                dev.append(rl.gen_sbm_device(ctx, n, k, 16.0, 20.0, seed=seed * 100003 + i, offset_bits=64))
+                truths.append((np.arange(n, dtype=np.int64) * k // n).astype(np.uint32))
+    db = rl.DeviceBatch.concat([d.csr for d in dev])
+    for d in dev:
+        d.close()
+    return db, truths
+
+
 def reduce_values(dist, values, op, device):
     """all_reduce of a list of numbers (op: "max" or "sum"); without a process group, the values."""
     if dist is None:
@@ -328,10 +354,11 @@ def batched_leg(ctx, count, steps, threads, stream, world=1, rank=0, dist=None):
     import torch
     import rak_lowmem as rl
     t0 = time.time()
-    graphs = batch_mix(count, 4, threads, keep=(lambda i: i % world == rank) if world > 1 else None)
-    mine = len(graphs)
-    hb = rl.HostBatch.concat(graphs, weighted=False)
-    log(f"[batched] {count} graphs, {hb.n} vertices, {hb.m} edges generated in {time.time() - t0:.1f}s")
+    hb, truths = batch_mix_device(ctx, count, 4, keep=(lambda i: i % world == rank) if world > 1 else None)
+    torch.cuda.synchronize()
+    mine = hb.graphs
+    gofs = hb.graph_offsets_host
+    log(f"[batched] {count} graphs, {hb.n} vertices, {hb.m} edges generated on the device in {time.time() - t0:.1f}s")
     b = rl.Batch(ctx, hb)
     out = torch.empty(hb.n, dtype=torch.int32, device="cuda")
     b.capture(out)
@@ -349,25 +376,25 @@ def batched_leg(ctx, count, steps, threads, stream, world=1, rank=0, dist=None):
     q_batch = b.modularity(out)
     # the loop: one resident graph per member (device views into the same arrays), one plain
     # rak_graph_run per graph
-    off_d = torch.from_numpy(hb.offsets).cuda()
-    tgt_d = torch.from_numpy(hb.targets.view(np.int32)).cuda()
+    off_d, tgt_d = hb.offsets, hb.targets
+    off_h = off_d.cpu().numpy()
     members, loop_out = [], []
     for i in range(mine):
-        a, z = int(hb.graph_offsets[i]), int(hb.graph_offsets[i + 1])
-        e_a = int(hb.offsets[a])
+        a, z = int(gofs[i]), int(gofs[i + 1])
+        e_a = int(off_h[a])
         off_i = (off_d[a:z + 1] - e_a).contiguous()
-        csr = rl.rak_csr(z - a, int(hb.offsets[z]) - e_a, 64, rl.DEVICE, off_i.data_ptr(),
+        csr = rl.rak_csr(z - a, int(off_h[z]) - e_a, 64, rl.DEVICE, off_i.data_ptr(),
                          tgt_d.data_ptr() + 4 * e_a if z > a else None, None)
         members.append((off_i, rl.ResidentGraph(ctx, csr, validate=0)))
     loop_lab = torch.empty_like(out)
     for i, (_, rg) in enumerate(members):   # warm-up: one run of every member
-        a, z = int(hb.graph_offsets[i]), int(hb.graph_offsets[i + 1])
+        a, z = int(gofs[i]), int(gofs[i + 1])
         if z > a:
             rg.run(loop_lab[a:z], label_order=1)
     e0.record(stream)
     for _ in range(steps):
         for i, (_, rg) in enumerate(members):
-            a, z = int(hb.graph_offsets[i]), int(hb.graph_offsets[i + 1])
+            a, z = int(gofs[i]), int(gofs[i + 1])
             if z > a:
                 rg.run(loop_lab[a:z], label_order=1)
     e1.record(stream)
@@ -376,11 +403,11 @@ def batched_leg(ctx, count, steps, threads, stream, world=1, rank=0, dist=None):
     q_loop = b.modularity(loop_lab)
     loop_np = loop_lab.cpu().numpy().view(np.uint32)
     nmis, nmis_loop = [], []
-    for i, g in enumerate(graphs):
-        if g.truth is not None:
-            a, z = int(hb.graph_offsets[i]), int(hb.graph_offsets[i + 1])
-            nmis.append(nmi(lab[a:z], g.truth))
-            nmis_loop.append(nmi(loop_np[a:z], g.truth))
+    for i, truth in enumerate(truths):
+        if truth is not None:
+            a, z = int(gofs[i]), int(gofs[i + 1])
+            nmis.append(nmi(lab[a:z], truth))
+            nmis_loop.append(nmi(loop_np[a:z], truth))
     for _, rg in members:
         rg.close()
     b.close()
@@ -541,7 +568,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--batch-graphs", type=int, default=256,
+    ap.add_argument("--batch-graphs", type=int, default=4096,
                     help="graphs in the batched-launch comparison (4096 = the full mix; 0 = skip)")
     ap.add_argument("--serving-seconds", type=float, default=2.0,
                     help="seconds of Poisson arrivals per rate in the serving comparison (0 = skip)")

@@ -118,7 +118,12 @@ typedef struct rak_options {
                                  the reference's rule. CPU sketch rules only. ASYNC: 2 [2]; SYNC
                                  and SYNC_SPLIT: 1 [1], 2 on request (deterministic) */
   int32_t tie_iterations;     /* 0: default [4]; iterations with hashed ties under tie_break 2 */
-  int64_t reserved[5];
+  int32_t edge_staging;       /* -1 or 0: default; 1: vertices and split-vertex chunks that a whole
+                                 warp scans read their edges from shared-memory tiles filled by bulk
+                                 copies (TMA, cp.async.bulk); 2: every lane loads its edges from
+                                 global memory. Results are the same either way. [2] */
+  int32_t reserved_i;
+  int64_t reserved[4];
 } rak_options;
 
 typedef struct rak_result {
@@ -376,6 +381,11 @@ rak_status rak_gen_rmat(int scale, double edge_factor, double a, double b, doubl
  * its graphs from files). */
 rak_status rak_gen_rmat_device(rak_ctx *ctx, int scale, double edge_factor, double a, double b, double c,
                                uint64_t seed, float w_lo, float w_hi, int32_t offset_bits, rak_csr *out);
+/* The planted-partition SBM of rak_gen_sbm built on ctx's device, bit-identical to it (unit weights:
+ * weights NULL; the planted block of vertex u is floor(u*k/n)). Needs about 16 bytes of device memory
+ * per sampled edge direction while it builds. No reference counterpart. */
+rak_status rak_gen_sbm_device(rak_ctx *ctx, int64_t n, int64_t k, double avg_degree, double in_out_ratio, uint64_t seed,
+                              int32_t offset_bits, rak_csr *out);
 rak_status rak_device_csr_free(rak_csr *g);
 /* The vertex order the reference's GPU path works in (inc/rakLowmemCuda.hxx:505-519, 563: vertex
  * ids partitioned by degree < 4, then the rest by degree < 128, with libstdc++'s std::partition

@@ -225,6 +225,7 @@ struct Resolved {
   double tol;
   long long timeout_ns;  // bound on each device-side wait
   int tie_until;         // iterations with hashed Misra-Gries ties
+  int stage;             // edge staging through shared memory
   Layout ly;
 };
 
@@ -276,6 +277,9 @@ rak_status resolve(rak_ctx *ctx, const rak_options *o, Resolved *r) {
   }
   if (o->tie_iterations < 0) { set_err(ctx, "tie_iterations must be >= 0"); return RAK_ERR_INVALID_ARGUMENT; }
   r->tie_until = tie == 2 ? (o->tie_iterations > 0 ? o->tie_iterations : rak::DEFAULT_TIE_ITERATIONS) : 0;
+  const int stg = o->edge_staging <= 0 ? rak::DEFAULT_EDGE_STAGING : o->edge_staging;
+  if (stg != 1 && stg != 2) { set_err(ctx, "edge_staging must be -1, 0, 1 or 2"); return RAK_ERR_INVALID_ARGUMENT; }
+  r->stage = stg == 1;
   r->timeout_ns = o->wait_timeout_ns > 0 ? (long long)o->wait_timeout_ns : rak::DEFAULT_WAIT_TIMEOUT_NS;
   r->start = o->start_iteration;
   r->validate = o->validate;
@@ -531,7 +535,7 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
   a.sk_keys = b.skk.as<uint32_t>(); a.sk_wts = b.skw.as<float>();
   a.stats = b.stats.as<unsigned long long>(); a.rs = b.rs.p;
   a.iters = r.iters; a.start_iter = r.start; a.tolerance = r.tol; a.pickless_step = r.pickless;
-  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until;
+  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until; a.stage = r.stage;
 
   // the kernel's module is loaded here, not inside the timed region
   if (r.iters > 0) RAK_TRY(ctx, rak::prepare_lpa(r.slots, r.mode, gr->off64, gr->wt == nullptr, false));
@@ -864,7 +868,7 @@ rak_status rak_graph_step(rak_ctx *ctx, rak_graph *gr, const rak_options *o, int
   a.sk_keys = b.skk.as<uint32_t>(); a.sk_wts = b.skw.as<float>();
   a.stats = b.stats.as<unsigned long long>(); a.rs = b.rs.p;
   a.iters = 1; a.start_iter = iteration; a.tolerance = r.tol; a.pickless_step = r.pickless;
-  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until;
+  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until; a.stage = r.stage;
   int grid = 0;
   RAK_TRY(ctx, rak::launch_lpa(a, r.slots, r.mode, gr->off64, st, &grid));
   unsigned long long s[rak::STATS_STRIDE] = {};
@@ -941,6 +945,41 @@ rak_status rak_gen_rmat_device(rak_ctx *ctx, int scale, double edge_factor, doub
   out->offsets = g.offsets;
   out->targets = g.targets;
   out->weights = g.weights;
+  return RAK_OK;
+}
+
+rak_status rak_gen_sbm_device(rak_ctx *ctx, int64_t n, int64_t k, double avg_degree, double in_out_ratio, uint64_t seed,
+                              int32_t offset_bits, rak_csr *out) {
+  cudaGetLastError();  // drop a stale error left by an unrelated failed call
+  if (!ctx || !out || n < 2 || n >= (int64_t(1) << 31) || k < 1 || k > n || !(avg_degree > 0) || !(in_out_ratio > 0) ||
+      (offset_bits != 32 && offset_bits != 64))
+    return RAK_ERR_INVALID_ARGUMENT;
+  std::memset(out, 0, sizeof(*out));
+  RAK_TRY(ctx, cudaSetDevice(ctx->device));
+  // the host generator's parameters (rak_gen.cpp, rak_gen_sbm)
+  const double s = double(n) / double(k);
+  const double fin = k == 1 ? 1.0 : in_out_ratio * (s - 1) / (in_out_ratio * (s - 1) + (double(n) - s));
+  const uint32_t fin24 = uint32_t(std::lround(fin * 16777216.0));
+  const int64_t samples = int64_t(std::llround(double(n) * avg_degree / 2.0));
+  rak::GenDeviceOut g{};
+  const cudaError_t e = rak::gen_sbm_device(n, k, samples, fin24, seed, offset_bits == 64, ctx->stream, &g);
+  if (e == cudaErrorInvalidValue) {
+    set_err(ctx, "more edges than 32-bit offsets can index");
+    return RAK_ERR_INVALID_ARGUMENT;
+  }
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    set_err(ctx, "device memory: the build needs about 16 bytes per sampled edge direction");
+    return RAK_ERR_OUT_OF_MEMORY;
+  }
+  RAK_TRY(ctx, e);
+  out->n = g.n;
+  out->m = g.m;
+  out->offset_bits = offset_bits;
+  out->location = RAK_DEVICE;
+  out->offsets = g.offsets;
+  out->targets = g.targets;
+  out->weights = nullptr;
   return RAK_OK;
 }
 
@@ -1138,7 +1177,7 @@ rak_status batch_enqueue(rak_ctx *ctx, rak_batch *b, const uint32_t *q, const Re
     a.giters = b->giters.as<int32_t>(); a.gchanged = b->gchanged.as<unsigned long long>();
     a.running = b->running.as<unsigned int>(); a.ngraphs = G; a.grid_cap = grid_cap;
     a.iters = r.iters; a.start_iter = r.start; a.tolerance = r.tol; a.pickless_step = r.pickless;
-    a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until;
+    a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until; a.stage = r.stage;
     int grid = 0;
     RAK_TRY(ctx, rak::launch_lpa(a, r.slots, r.mode, true, st, &grid, true));
   }

@@ -59,6 +59,8 @@ constexpr int64_t DEFAULT_HUB_CHUNK = 8192;
 constexpr int64_t MAX_LANE_MAX = 1024;
 // Iterations with hashed ties (rak_options.tie_break 2) when rak_options.tie_iterations is 0.
 constexpr int DEFAULT_TIE_ITERATIONS = 4;
+// Edge staging (rak_options.edge_staging) when the option is 0: 1 on, 2 off.
+constexpr int DEFAULT_EDGE_STAGING = 2;
 // Bound on each device-side wait when rak_options.wait_timeout_ns is 0.
 constexpr long long DEFAULT_WAIT_TIMEOUT_NS = 20LL * 1000 * 1000 * 1000;
 
@@ -114,6 +116,7 @@ struct LpaArgs {
   int mark_test;                // neighbour marking reads a flag before storing it (mark_test_for)
   int gpu_rule;                 // synchronous split mode: the reference GPU sketch rules (else CPU)
   int tie_until;                // iterations l < tie_until break Misra-Gries ties by hash (CPU rules)
+  int stage;                    // warp-wide edge ranges read through shared-memory tiles (bulk copies)
   int iters;
   int start_iter;
   double tolerance;
@@ -184,6 +187,9 @@ struct GenDeviceOut {
 };
 cudaError_t gen_rmat_device(int scale, int64_t samples, uint64_t seed, uint32_t tA, uint32_t tAB, uint32_t tABC,
                             bool weighted, float w_lo, float w_hi, bool off64, cudaStream_t st, GenDeviceOut *out);
+// Planted-partition SBM on the device (rak_gen_device.cu), the samples of rak_gen_sbm.
+cudaError_t gen_sbm_device(int64_t n, int64_t k, int64_t samples, uint32_t fin24, uint64_t seed, bool off64,
+                           cudaStream_t st, GenDeviceOut *out);
 // One graph to pack into a batch CSR from device memory (k_gather_graphs).
 struct GatherItem {
   const void *off;       // n + 1 offsets, int64 if off64 else int32

@@ -196,32 +196,30 @@ __device__ __forceinline__ void mark_item(const LpaArgs &a, uint32_t u, int64_t 
 
 // ---- edge tiles staged in shared memory by the bulk-copy engine (TMA) -------------------------
 //
-// Lane groups (G lanes per vertex, regions 1-5) and split-vertex chunks (region 0, G = 32) scan
-// contiguous edge ranges. Instead of every lane loading its targets and weights from global memory
-// a few edges ahead, each group's range is copied tile by tile into shared memory with 1-D bulk
-// copies (cp.async.bulk, completion counted in bytes on an mbarrier), STG_STAGES tiles ahead of the
-// lanes, and the lanes read their edges there. Lane s of a group still accumulates edges eb+s,
-// eb+s+G, ... in that order, so sketches are bit-identical to scan_range's. Bulk copies need
-// 16-byte aligned addresses and sizes: the few edges before the first aligned address of a range
-// and after its last one are read from global memory directly, so no copy reads outside [eb, ee).
-// The source is always this GPU's own memory; no copy uses a multicast form.
+// Vertices scanned by a whole warp -- lane groups of 32 (region 1) and split-vertex chunks
+// (region 0) -- read one contiguous edge range. With LpaArgs::stage the range is copied tile by
+// tile into shared memory with 1-D bulk copies (cp.async.bulk, completion counted in bytes on an
+// mbarrier), one tile ahead of the lanes, and the lanes read their edges there instead of loading
+// them from global memory. Lane s still accumulates edges eb+s, eb+s+32, ... in that order, so the
+// sketches are bit-identical to scan_range's. Bulk copies need 16-byte aligned addresses and sizes:
+// the few edges before the range's first aligned address and after its last one are read from
+// global memory directly, so no copy reads outside [eb, ee). The source is always this GPU's own
+// memory; no copy uses a multicast form.
 #ifndef RAK_STAGE
 #define RAK_STAGE 1
 #endif
 constexpr int LPA_WARPS = 8;      // warps per block (256 threads)
-constexpr int STG_TILE = 256;     // edges per warp per stage, divided among the warp's lane groups
-constexpr int STG_BUF = STG_TILE + 64;  // per stage: group slices padded by 4 edges (bank spread)
-constexpr int STG_STAGES = 3;     // tiles in flight per warp
-constexpr int STG_B = 4;          // edges per lane per gather batch from a staged tile
+constexpr int STG_TILE = 512;     // edges per tile (16 per lane)
+constexpr int STG_STAGES = 2;     // tiles per warp: one in use, one in flight
 
-// Dynamic shared memory of an lpa_run block that stages tiles: per warp STG_STAGES buffers of
-// targets (and of weights, for weighted graphs), then one mbarrier per buffer.
+// Dynamic shared memory of an lpa_run block that stages tiles: per warp STG_STAGES tiles of
+// targets (and of weights, for weighted graphs), then one mbarrier per tile buffer.
 __host__ __device__ constexpr size_t stage_bytes(bool unit) {
-  return size_t(LPA_WARPS) * STG_STAGES * STG_BUF * 4 * (unit ? 1 : 2) + size_t(LPA_WARPS) * STG_STAGES * 8;
+  return size_t(LPA_WARPS) * STG_STAGES * STG_TILE * 4 * (unit ? 1 : 2) + size_t(LPA_WARPS) * STG_STAGES * 8;
 }
 
 struct StageCtx {
-  uint32_t *t;     // this warp's target buffers (STG_STAGES x STG_BUF)
+  uint32_t *t;     // this warp's target buffers (STG_STAGES x STG_TILE)
   float *w;        // this warp's weight buffers (weighted graphs)
   uint32_t bar;    // shared-memory address of this warp's first mbarrier
   uint32_t phase;  // per buffer, the parity of the next completion to wait for (warp-uniform)
@@ -246,19 +244,11 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// 1-D bulk copy global -> this CTA's shared memory, completing `bytes` on the mbarrier; the edge
-// stream keeps its L2 evict-first policy.
+// 1-D bulk copy global -> this CTA's shared memory, completing `bytes` on the mbarrier.
 __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
-#if RAK_STREAM_HINT
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
-      ::"r"(dst), "l"(src), "r"(bytes), "r"(bar), "l"(l2_stream_policy())
-      : "memory");
-#else
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
                : "memory");
-#endif
 }
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
@@ -280,91 +270,100 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, RunStat
   return true;
 }
 
-// Issues tile k of a group's copy range [cs, ce) (tiles of `slice` edges) into buffer k % STG_STAGES.
-// Called by every lane of the warp; lane 0 arms the buffer's mbarrier with the bytes of all
-// groups' copies, then each group's first lane starts its copies.
+// Lane 0 starts the copy of tile k of [cs, ce) into buffer k % STG_STAGES (all lanes call this).
 template <bool UNIT>
-__device__ __forceinline__ void stage_issue(const StageCtx &sc, int k, int64_t cs, int64_t ce, int slice, int off,
-                                            bool leader, const uint32_t *tgt, const float *wt) {
+__device__ __forceinline__ void stage_issue(const StageCtx &sc, int k, int64_t cs, int64_t ce, const uint32_t *tgt,
+                                            const float *wt) {
   const int buf = k % STG_STAGES;
-  const int64_t tb = cs + int64_t(k) * slice;
-  const int64_t te = tb + slice < ce ? tb + slice : ce;
+  const int64_t tb = cs + int64_t(k) * STG_TILE;
+  const int64_t te = tb + STG_TILE < ce ? tb + STG_TILE : ce;
   const uint32_t bytes = te > tb ? uint32_t(te - tb) * 4u : 0u;
-  const uint32_t total = __reduce_add_sync(FULL, leader ? bytes : 0u) * (UNIT ? 1u : 2u);
   const uint32_t bar = sc.bar + 8u * uint32_t(buf);
   fence_proxy_async_smem();  // this buffer's earlier reads come before the copy that refills it
   __syncwarp();
-  if ((threadIdx.x & 31) == 0) mbar_expect_arrive(bar, total);
-  __syncwarp();
-  if (leader && bytes) {
-    bulk_g2s(smem_u32(sc.t + buf * STG_BUF + off), tgt + tb, bytes, bar);
-    if constexpr (!UNIT) bulk_g2s(smem_u32(sc.w + buf * STG_BUF + off), wt + tb, bytes, bar);
+  if ((threadIdx.x & 31) == 0) {
+    mbar_expect_arrive(bar, bytes * (UNIT ? 1u : 2u));
+    if (bytes) {
+      bulk_g2s(smem_u32(sc.t + buf * STG_TILE), tgt + tb, bytes, bar);
+      if constexpr (!UNIT) bulk_g2s(smem_u32(sc.w + buf * STG_TILE), wt + tb, bytes, bar);
+    }
   }
 }
 
-// Staged form of scan_range for the lane groups of a warp: lane s of the group of G lanes that
-// owns u accumulates edges eb+s, eb+s+G, ... < ee in that order. Every lane of the warp calls it
-// (the tile loop is warp-uniform); a group with nothing to scan passes eb == ee.
+// Staged form of scan_range(sk, u, eb + lane, ee, 32, ...) for a range scanned by the whole warp.
+// Every lane calls it with the same range (eb == ee: nothing to scan).
 template <int S, bool UNIT, int RULE>
-__device__ __forceinline__ void staged_scan(Sketch<S> &sk, StageCtx &sc, uint32_t u, int64_t eb, int64_t ee, int G,
-                                            int s, const uint32_t *tgt, const float *wt, const uint32_t *vin,
-                                            uint32_t base, RunState *rs, long long timeout_ns) {
+__device__ __forceinline__ void staged_scan(Sketch<S> &sk, StageCtx &sc, uint32_t u, int64_t eb, int64_t ee,
+                                            const uint32_t *tgt, const float *wt, const uint32_t *vin, uint32_t base,
+                                            RunState *rs, long long timeout_ns) {
+  constexpr int B = RAK_SCAN_BATCH;
   const int lane = threadIdx.x & 31;
-  const int slice = STG_TILE / 32 * G;                                // edges per group per tile
-  const int off = (lane / G) * (slice + (G < 32 ? 4 : 0));            // the group's part of a buffer
   // Copies cover [cs, ce): cs the first edge at a 16-byte aligned address at or after eb, ce the
-  // last such boundary at or before ee. Tile k copies [cs + k*slice, min(cs + (k+1)*slice, ce));
-  // the lanes take edges before cs in tile 0 and after ce in the group's last tile from global.
+  // last such boundary at or before ee. Tile k copies [cs + k*STG_TILE, min(cs + (k+1)*STG_TILE, ce));
+  // the lanes take edges before cs in tile 0 and after ce in the last tile from global memory.
   int64_t cs = eb + int64_t(((16u - (uint32_t(reinterpret_cast<uintptr_t>(tgt + eb)) & 15u)) & 15u) >> 2);
   if (cs > ee) cs = ee;
   const int64_t ce = cs + ((ee - cs) & ~int64_t(3));
-  int nt = ee > eb ? int((ee - cs + slice - 1) / slice) : 0;
+  int nt = ee > eb ? int((ee - cs + STG_TILE - 1) / STG_TILE) : 0;
   if (ee > eb && nt < 1) nt = 1;
-  const int ntiles = int(__reduce_max_sync(FULL, unsigned(nt)));
-  const bool leader = s == 0;
-  for (int k = 0; k < STG_STAGES && k < ntiles; ++k)
-    stage_issue<UNIT>(sc, k, cs, k < nt ? ce : cs, slice, off, leader, tgt, wt);
-  int rel = int(eb - cs) + s;   // the lane's next edge, relative to the current tile's first edge
-  for (int k = 0; k < ntiles; ++k) {
+  for (int k = 0; k < STG_STAGES && k < nt; ++k) stage_issue<UNIT>(sc, k, cs, ce, tgt, wt);
+  int rel = int(eb - cs) + lane;   // the lane's next edge, relative to the current tile's first edge
+  for (int k = 0; k < nt; ++k) {
     const int buf = k % STG_STAGES;
     const bool ok = mbar_wait(sc.bar + 8u * uint32_t(buf), (sc.phase >> buf) & 1u, rs, timeout_ns);
     sc.phase ^= 1u << buf;
-    const int64_t tb = cs + int64_t(k) * slice;
-    // relative bounds: the tile's edges end at hi (the group's last tile takes the tail), the
-    // copied ones at se
-    const int hi = k + 1 >= nt ? int(ee - tb) : (slice < ee - tb ? slice : int(ee - tb));
-    const int se = ok ? (slice < ce - tb ? slice : int(ce - tb)) : 0;
-    const uint32_t *bt = sc.t + buf * STG_BUF + off;
-    const float *bw = sc.w + buf * STG_BUF + off;
-    while (rel < hi) {
-      const int left = (hi - rel + G - 1) / G;
-      const int take = left < STG_B ? left : STG_B;
-      uint32_t t[STG_B];
-      float w[STG_B];
+    const int64_t tb = cs + int64_t(k) * STG_TILE;
+    const uint32_t *bt = sc.t + buf * STG_TILE;
+    const float *bw = sc.w + buf * STG_TILE;
+    const bool whole = ok && k > 0 && tb + STG_TILE <= ce;   // every edge of the tile is in shared memory
+    if (whole) {
 #pragma unroll
-      for (int j = 0; j < STG_B; ++j) {
-        const int x = rel + j * G;
-        t[j] = u;
-        w[j] = 0.0f;
-        if (j < take) {
-          const bool in = x >= 0 && x < se;
-          t[j] = base + (in ? bt[x] : ld_edge(tgt + (tb + x)));
-          if constexpr (UNIT) w[j] = 1.0f;
-          else w[j] = in ? bw[x] : ld_weight(wt + (tb + x));
+      for (int b0 = 0; b0 < STG_TILE / 32; b0 += B) {
+        uint32_t t[B], c[B];
+        float w[B];
+#pragma unroll
+        for (int j = 0; j < B; ++j) {
+          const int x = rel + (b0 + j) * 32;
+          t[j] = base + bt[x];
+          w[j] = UNIT ? 1.0f : bw[x];
         }
+#pragma unroll
+        for (int j = 0; j < B; ++j) c[j] = vin[t[j]];
+#pragma unroll
+        for (int j = 0; j < B; ++j)
+          if (t[j] != u) sk_acc<S, RULE>(sk, c[j], w[j]);
       }
-      uint32_t c[STG_B];
+      rel += STG_TILE;
+    } else {
+      // the first or last tile (or a tile whose copy gave up): edges outside the copy from global
+      const int hi = k + 1 >= nt ? int(ee - tb) : STG_TILE;
+      const int se = ok ? (tb + STG_TILE < ce ? STG_TILE : int(ce - tb)) : 0;
+      while (rel < hi) {
+        uint32_t t[B], c[B];
+        float w[B];
 #pragma unroll
-      for (int j = 0; j < STG_B; ++j) c[j] = vin[t[j]];
+        for (int j = 0; j < B; ++j) {
+          const int x = rel + j * 32;
+          t[j] = u;
+          w[j] = 0.0f;
+          if (x < hi) {
+            const bool in = x >= 0 && x < se;
+            t[j] = base + (in ? bt[x] : ld_edge(tgt + (tb + x)));
+            if constexpr (UNIT) w[j] = 1.0f;
+            else w[j] = in ? bw[x] : ld_weight(wt + (tb + x));
+          }
+        }
 #pragma unroll
-      for (int j = 0; j < STG_B; ++j)
-        if (t[j] != u) sk_acc<S, RULE>(sk, c[j], w[j]);
-      rel += take * G;
+        for (int j = 0; j < B; ++j) c[j] = vin[t[j]];
+#pragma unroll
+        for (int j = 0; j < B; ++j)
+          if (t[j] != u) sk_acc<S, RULE>(sk, c[j], w[j]);
+        rel += B * 32;
+      }
     }
-    rel -= slice;
+    rel -= STG_TILE;
     __syncwarp();
-    if (k + STG_STAGES < ntiles)
-      stage_issue<UNIT>(sc, k + STG_STAGES, cs, k + STG_STAGES < nt ? ce : cs, slice, off, leader, tgt, wt);
+    if (k + STG_STAGES < nt) stage_issue<UNIT>(sc, k + STG_STAGES, cs, ce, tgt, wt);
   }
 }
 
@@ -537,8 +536,8 @@ __device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, 
   if constexpr (MODE == MODE_SYNC) {
     if (active) exact_group_scan<S, UNIT>(sk, u, eb, ee, G, grp, s, S > 1 && a.rescan, g.tgt, g.wt, vin, base);
   } else {
-    if (sc.on)
-      staged_scan<S, UNIT, RULE>(sk, sc, u, active ? eb : 0, active ? ee : 0, G, s, g.tgt, g.wt, vin, base,
+    if (sc.on && G == 32)   // one vertex per warp: the warp's range is uniform
+      staged_scan<S, UNIT, RULE>(sk, sc, u, active ? eb : 0, active ? ee : 0, g.tgt, g.wt, vin, base,
                                  static_cast<RunState *>(a.rs), a.timeout_ns);
     else if (active)
       scan_range<S, UNIT, RULE>(sk, u, eb + s, ee, G, g.tgt, g.wt, vin, base);
@@ -629,7 +628,7 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
     sk_clear<S, RULE>(sk, d0);
     const int64_t cb = eb + j * a.hub_chunk, ce = cb + a.hub_chunk < ee ? cb + a.hub_chunk : ee;
     if (sc.on)   // active is the same on every lane
-      staged_scan<S, UNIT, RULE>(sk, sc, u, active ? cb : 0, active ? ce : 0, 32, lane, g.tgt, g.wt, vin, base,
+      staged_scan<S, UNIT, RULE>(sk, sc, u, active ? cb : 0, active ? ce : 0, g.tgt, g.wt, vin, base,
                                  static_cast<RunState *>(a.rs), a.timeout_ns);
     else if (active)
       scan_range<S, UNIT, RULE>(sk, u, cb + lane, ce, 32, g.tgt, g.wt, vin, base);
@@ -719,13 +718,13 @@ __global__ void __launch_bounds__(256, RAK_MIN_BLOCKS) lpa_run(const LpaArgs a) 
   if constexpr (MODE != MODE_SYNC && RAK_STAGE) {
     extern __shared__ __align__(128) unsigned char lpa_dsm[];
     const int w = threadIdx.x >> 5;
-    constexpr size_t tbytes = size_t(LPA_WARPS) * STG_STAGES * STG_BUF * 4;
-    sc.t = reinterpret_cast<uint32_t *>(lpa_dsm) + size_t(w) * STG_STAGES * STG_BUF;
-    sc.w = UNIT ? nullptr : reinterpret_cast<float *>(lpa_dsm + tbytes) + size_t(w) * STG_STAGES * STG_BUF;
+    constexpr size_t tbytes = size_t(LPA_WARPS) * STG_STAGES * STG_TILE * 4;
+    sc.t = reinterpret_cast<uint32_t *>(lpa_dsm) + size_t(w) * STG_STAGES * STG_TILE;
+    sc.w = UNIT ? nullptr : reinterpret_cast<float *>(lpa_dsm + tbytes) + size_t(w) * STG_STAGES * STG_TILE;
     sc.bar = smem_u32(lpa_dsm + tbytes * (UNIT ? 1 : 2)) + 8u * uint32_t(w * STG_STAGES);
     sc.phase = 0;
     // targets and weights must share their 16-byte alignment (one copy range serves both)
-    sc.on = UNIT || ((reinterpret_cast<uintptr_t>(a.tgt) ^ reinterpret_cast<uintptr_t>(a.wt)) & 15u) == 0;
+    sc.on = a.stage && (UNIT || ((reinterpret_cast<uintptr_t>(a.tgt) ^ reinterpret_cast<uintptr_t>(a.wt)) & 15u) == 0);
     if (lane < STG_STAGES) mbar_init(sc.bar + 8u * uint32_t(lane), 1);
     fence_mbar_init();
     __syncwarp();

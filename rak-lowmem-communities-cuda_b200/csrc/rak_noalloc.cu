@@ -136,7 +136,7 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   if (order_kind == 2 && sync) return RAK_ERR_UNSUPPORTED;
   const int iters = o->max_iterations;
   if (iters < 0 || iters > 1024 || !(o->tolerance >= 0) || o->wait_timeout_ns < 0) return RAK_ERR_INVALID_ARGUMENT;
-  if (o->tie_break > 2 || o->tie_iterations < 0) return RAK_ERR_INVALID_ARGUMENT;
+  if (o->tie_break > 2 || o->tie_iterations < 0 || o->edge_staging > 2) return RAK_ERR_INVALID_ARGUMENT;
   if (o->tie_break == 2 && o->sketch_rule == 2) return RAK_ERR_UNSUPPORTED;
   Layout ly;
   ly.lane_max = o->lane_max > 0 ? o->lane_max : DEFAULT_LANE_MAX;
@@ -290,6 +290,7 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   // ties as in rak_lowmem_cuda: hashed during the first iterations of asynchronous runs
   const int tie = o->tie_break <= 0 ? (mode == RAK_MODE_ASYNC && !a.gpu_rule ? 2 : 1) : o->tie_break;
   a.tie_until = tie == 2 ? (o->tie_iterations > 0 ? o->tie_iterations : DEFAULT_TIE_ITERATIONS) : 0;
+  a.stage = (o->edge_staging <= 0 ? DEFAULT_EDGE_STAGING : o->edge_staging) == 1;
   a.timeout_ns = o->wait_timeout_ns > 0 ? (long long)o->wait_timeout_ns : DEFAULT_WAIT_TIMEOUT_NS;
   if (iters > 0) {
     int grid = 0;

@@ -45,7 +45,7 @@ class rak_options(C.Structure):
                 ("compute_modularity", C.c_int32), ("start_iteration", C.c_int32),
                 ("initial_flags", C.c_void_p), ("sketch_rule", C.c_int32), ("label_order", C.c_int32),
                 ("wait_timeout_ns", C.c_int64), ("tie_break", C.c_int32), ("tie_iterations", C.c_int32),
-                ("reserved", C.c_int64 * 5)]
+                ("edge_staging", C.c_int32), ("reserved_i", C.c_int32), ("reserved", C.c_int64 * 4)]
 
 
 class rak_result(C.Structure):
@@ -148,6 +148,8 @@ _sig("rak_gen_lattice", C.c_int, C.c_int64, C.c_int64, C.c_double, C.c_double, C
 _sig("rak_host_csr_free", None, C.POINTER(rak_host_csr))
 _sig("rak_gen_rmat_device", C.c_int, P, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint64,
      C.c_float, C.c_float, C.c_int32, C.POINTER(rak_csr))
+_sig("rak_gen_sbm_device", C.c_int, P, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_uint64, C.c_int32,
+     C.POINTER(rak_csr))
 _sig("rak_device_csr_free", C.c_int, C.POINTER(rak_csr))
 _sig("rak_reference_vertex_order", C.c_int, P, C.POINTER(rak_csr), P)
 _sig("rak_batch_reference_vertex_order", C.c_int, P, P, P)
@@ -339,6 +341,14 @@ def gen_rmat_device(ctx, scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=42,
     c_ = rak_csr()
     _check(_lib.rak_gen_rmat_device(ctx.handle, scale, edge_factor, a, b, c, seed, w_lo, w_hi, offset_bits,
                                     C.byref(c_)), ctx.handle)
+    return DeviceGraph(c_)
+
+
+def gen_sbm_device(ctx, n, k, avg_degree=16.0, in_out_ratio=20.0, seed=42, offset_bits=64) -> DeviceGraph:
+    """rak_gen_sbm_device: the graph gen_sbm builds, built on ctx's device."""
+    c_ = rak_csr()
+    _check(_lib.rak_gen_sbm_device(ctx.handle, n, k, avg_degree, in_out_ratio, seed, offset_bits, C.byref(c_)),
+           ctx.handle)
     return DeviceGraph(c_)
 
 
@@ -563,11 +573,72 @@ class HostBatch:
                              self.weights.ctypes.data if self.weights is not None else None)
 
 
+class DeviceBatch:
+    """Graphs concatenated into one CSR in device memory (torch CUDA tensors): graph_offsets and
+    offsets int64, targets int32 (ids local to each graph), weights float32 or None. Built from
+    device graphs by concat without a host round trip of the edges."""
+
+    def __init__(self, graph_offsets, offsets, targets, weights=None):
+        self.graph_offsets, self.offsets, self.targets, self.weights = graph_offsets, offsets, targets, weights
+        self.graphs = int(graph_offsets.numel()) - 1
+        self.n = int(graph_offsets[-1].item())
+        self.m = int(offsets[-1].item())
+        self.graph_offsets_host = graph_offsets.cpu().numpy()
+
+    @staticmethod
+    def concat(graphs) -> "DeviceBatch":
+        """Packs device graphs (rak_csr of location DEVICE, unit weights) into one batch."""
+        import torch
+        go = np.zeros(len(graphs) + 1, np.int64)
+        go[1:] = np.cumsum([int(g.n) for g in graphs])
+        eo = np.zeros(len(graphs) + 1, np.int64)
+        eo[1:] = np.cumsum([int(g.m) for g in graphs])
+        off = torch.empty(int(go[-1]) + 1, dtype=torch.int64, device="cuda")
+        tgt = torch.empty(max(int(eo[-1]), 1), dtype=torch.int32, device="cuda")
+        for i, g in enumerate(graphs):
+            n, m = int(g.n), int(g.m)
+            off_i = _device_view(g.offsets, n + 1, torch.int64 if g.offset_bits == 64 else torch.int32)
+            off[go[i]:go[i + 1]] = off_i[:n].to(torch.int64) + int(eo[i])
+            if m:
+                tgt[eo[i]:eo[i + 1]] = _device_view(g.targets, m, torch.int32)
+        off[-1] = int(eo[-1])
+        return DeviceBatch(torch.from_numpy(go).cuda(), off, tgt[:int(eo[-1])])
+
+    def csr(self) -> rak_batch_csr:
+        return rak_batch_csr(self.graphs, self.n, self.m, DEVICE, 0, self.graph_offsets.data_ptr(),
+                             self.offsets.data_ptr(), self.targets.data_ptr() if self.m else None,
+                             self.weights.data_ptr() if self.weights is not None else None)
+
+
+def _device_view(ptr, count, dtype):
+    """A torch CUDA tensor over `count` elements of device memory at ptr (not owned)."""
+    import torch
+    if count == 0:
+        return torch.empty(0, dtype=dtype, device="cuda")
+    esz = torch.empty(0, dtype=dtype).element_size()
+    return _ViewHolder.wrap(ptr, count * esz).view(dtype)[:count]
+
+
+class _ViewHolder:
+    """Wraps raw device memory as a uint8 torch tensor through __cuda_array_interface__."""
+
+    def __init__(self, ptr, nbytes):
+        self.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+    @staticmethod
+    def wrap(ptr, nbytes):
+        import torch
+        return torch.as_tensor(_ViewHolder(ptr, nbytes), device="cuda")
+
+
 class Batch:
     """A device-resident batch of graphs (rak_batch): one persistent launch runs them all."""
 
-    def __init__(self, ctx: Context, host_batch: HostBatch, **opts):
+    def __init__(self, ctx: Context, host_batch, **opts):
+        """host_batch: a HostBatch, or a DeviceBatch (bound in place, not copied)."""
         self.ctx = ctx
+        self._keep = host_batch
         self.graphs = host_batch.graphs
         self.n = host_batch.n
         self._b = P()

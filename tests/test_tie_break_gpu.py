@@ -68,11 +68,12 @@ def test_sync_steps_with_hashed_ties(ctx):
     rg.close()
 
 
-@pytest.mark.parametrize("slots", [2, 8, 16])
-def test_async_default_valid(ctx, slots):
+@pytest.mark.parametrize("slots,q_min", [(2, 0.3), (8, 0.6), (16, 0.6)])
+def test_async_default_valid(ctx, slots, q_min):
+    """Two slots cannot hold a degree-4 neighbourhood, so its bound is lower."""
     g = rl.gen_lattice(300, 200, 0.05, 0.01, seed=12)
     lab, res = ctx.lowmem(g, slots=slots, compute_modularity=1)
-    assert lab.max() < g.n and res.iterations >= 1 and res.modularity > 0.4
+    assert lab.max() < g.n and res.iterations >= 1 and res.modularity > q_min
 
 
 def test_option_errors(ctx):
