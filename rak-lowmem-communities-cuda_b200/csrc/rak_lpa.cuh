@@ -338,7 +338,11 @@ __device__ __forceinline__ void staged_scan(Sketch<S> &sk, StageCtx &sc, uint32_
       // the first or last tile (or a tile whose copy gave up): edges outside the copy from global
       const int hi = k + 1 >= nt ? int(ee - tb) : STG_TILE;
       const int se = ok ? (tb + STG_TILE < ce ? STG_TILE : int(ce - tb)) : 0;
+      // the lane consumes only its edges below hi, so that it enters the next tile at an offset
+      // in [0, 32): the whole-tile path reads offsets up to that offset + STG_TILE - 32
       while (rel < hi) {
+        const int left = (hi - rel + 31) >> 5;
+        const int take = left < B ? left : B;
         uint32_t t[B], c[B];
         float w[B];
 #pragma unroll
@@ -346,7 +350,7 @@ __device__ __forceinline__ void staged_scan(Sketch<S> &sk, StageCtx &sc, uint32_
           const int x = rel + j * 32;
           t[j] = u;
           w[j] = 0.0f;
-          if (x < hi) {
+          if (j < take) {
             const bool in = x >= 0 && x < se;
             t[j] = base + (in ? bt[x] : ld_edge(tgt + (tb + x)));
             if constexpr (UNIT) w[j] = 1.0f;
@@ -358,7 +362,7 @@ __device__ __forceinline__ void staged_scan(Sketch<S> &sk, StageCtx &sc, uint32_
 #pragma unroll
         for (int j = 0; j < B; ++j)
           if (t[j] != u) sk_acc<S, RULE>(sk, c[j], w[j]);
-        rel += B * 32;
+        rel += take * 32;
       }
     }
     rel -= STG_TILE;
