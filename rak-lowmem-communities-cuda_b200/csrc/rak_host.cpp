@@ -538,7 +538,7 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
   a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until; a.stage = r.stage;
 
   // the kernel's module is loaded here, not inside the timed region
-  if (r.iters > 0) RAK_TRY(ctx, rak::prepare_lpa(r.slots, r.mode, gr->off64, gr->wt == nullptr, false));
+  if (r.iters > 0) RAK_TRY(ctx, rak::prepare_lpa(r.slots, r.mode, gr->off64, gr->wt == nullptr, false, r.stage));
   // Labels as positions in the reference GPU path's vertex order (inc/rakLowmemCuda.hxx:563,
   // 591-592), so that its pickless rule compares the same label order; turned back into vertex ids
   // after the run. The order depends on degrees only: built once per graph.
@@ -1097,7 +1097,7 @@ namespace {
 rak_status batch_prepare(rak_ctx *ctx, rak_batch *b, const Resolved &r) {
   rak_graph *gr = b->g;
   if (!same_layout(gr->ly, r.ly)) RAK_CHECK(build_plan(ctx, gr, r.ly, nullptr));
-  if (r.iters > 0) RAK_TRY(ctx, rak::prepare_lpa(r.slots, r.mode, true, gr->wt == nullptr, true));
+  if (r.iters > 0) RAK_TRY(ctx, rak::prepare_lpa(r.slots, r.mode, true, gr->wt == nullptr, true, r.stage));
   const int64_t n = gr->n, G = b->ngraphs;
   const bool sync = r.mode != RAK_MODE_ASYNC;
   const int iters = std::max(r.iters, 1);

@@ -140,7 +140,7 @@ cudaError_t launch_lpa(const LpaArgs &a, int slots, int mode, bool off64, cudaSt
 template <int S>
 cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, bool batch, cudaStream_t st, int *grid_out);
 template <int S>
-cudaError_t resolve_lpa_slots(int mode, bool off64, bool unit, bool batch, const void **fn, int *per_sm);
+cudaError_t resolve_lpa_slots(int mode, bool off64, bool unit, bool batch, bool stage, const void **fn, int *per_sm);
 // Whether neighbour marking inside work items reads each flag before storing it. Measured to pay
 // for the Boyer-Moore sketch on graphs of 2^20 vertices and more whose average degree is 8 or more
 // (R-MAT s22-s24: 25-35% faster; SBM 4M: 5%), where many moved vertices mark the same hub flags,
@@ -150,7 +150,7 @@ inline int mark_test_for(int slots, int64_t n, int64_t m) {
   return slots == 1 && n >= (int64_t(1) << 20) && m >= 8 * n ? 1 : 0;
 }
 // Loads and resolves the kernel a run will launch (outside its timed region).
-cudaError_t prepare_lpa(int slots, int mode, bool off64, bool unit, bool batch);
+cudaError_t prepare_lpa(int slots, int mode, bool off64, bool unit, bool batch, bool stage);
 
 // Plan and utility kernels (rak_kernels.cu).
 cudaError_t launch_validate(const void *off, bool off64, const uint32_t *tgt, int64_t n, int64_t m,

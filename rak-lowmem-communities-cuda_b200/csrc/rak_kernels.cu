@@ -528,15 +528,15 @@ cudaError_t launch_modularity(const void *off, bool off64, const uint32_t *tgt, 
   return cudaGetLastError();
 }
 
-cudaError_t prepare_lpa(int slots, int mode, bool off64, bool unit, bool batch) {
+cudaError_t prepare_lpa(int slots, int mode, bool off64, bool unit, bool batch, bool stage) {
   const void *fn = nullptr;
   int per_sm = 0;
   switch (slots) {
-    case 1: return resolve_lpa_slots<1>(mode, off64, unit, batch, &fn, &per_sm);
-    case 2: return resolve_lpa_slots<2>(mode, off64, unit, batch, &fn, &per_sm);
-    case 4: return resolve_lpa_slots<4>(mode, off64, unit, batch, &fn, &per_sm);
-    case 8: return resolve_lpa_slots<8>(mode, off64, unit, batch, &fn, &per_sm);
-    case 16: return resolve_lpa_slots<16>(mode, off64, unit, batch, &fn, &per_sm);
+    case 1: return resolve_lpa_slots<1>(mode, off64, unit, batch, stage, &fn, &per_sm);
+    case 2: return resolve_lpa_slots<2>(mode, off64, unit, batch, stage, &fn, &per_sm);
+    case 4: return resolve_lpa_slots<4>(mode, off64, unit, batch, stage, &fn, &per_sm);
+    case 8: return resolve_lpa_slots<8>(mode, off64, unit, batch, stage, &fn, &per_sm);
+    case 16: return resolve_lpa_slots<16>(mode, off64, unit, batch, stage, &fn, &per_sm);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -209,7 +209,7 @@ __device__ __forceinline__ void mark_item(const LpaArgs &a, uint32_t u, int64_t 
 #define RAK_STAGE 1
 #endif
 constexpr int LPA_WARPS = 8;      // warps per block (256 threads)
-constexpr int STG_TILE = 512;     // edges per tile (16 per lane)
+constexpr int STG_TILE = 256;     // edges per tile (8 per lane): 16 KB of tiles per block (32 KB weighted)
 constexpr int STG_STAGES = 2;     // tiles per warp: one in use, one in flight
 
 // Dynamic shared memory of an lpa_run block that stages tiles: per warp STG_STAGES tiles of
@@ -863,14 +863,19 @@ __global__ void __launch_bounds__(256, RAK_MIN_BLOCKS) lpa_run(const LpaArgs a) 
   }
 }
 
-// Dynamic shared memory of an lpa_run launch: the staged edge tiles of the modes that use them.
-inline size_t lpa_dynamic_smem(int mode, bool unit) { return (mode != MODE_SYNC && RAK_STAGE) ? stage_bytes(unit) : 0; }
+// Dynamic shared memory of an lpa_run launch: the staged edge tiles, when the launch stages edges.
+// Without staging the launch takes none, which leaves the SM's L1 cache its full size for the
+// label gathers (shared memory and L1 share the SM's 256 KB).
+inline size_t lpa_dynamic_smem(int mode, bool unit, bool stage) {
+  return (mode != MODE_SYNC && RAK_STAGE && stage) ? stage_bytes(unit) : 0;
+}
 
 // The kernel instantiation for a launch and its resident blocks per SM, cached per (function,
 // device). The first query of an instantiation loads its module (CUDA loads modules lazily, which
 // can take a millisecond), so runs resolve before their timed region (prepare_lpa).
 template <int S>
-cudaError_t resolve_lpa_slots(int mode, bool off64, bool unit, bool batch, const void **fn_out, int *per_sm_out) {
+cudaError_t resolve_lpa_slots(int mode, bool off64, bool unit, bool batch, bool stage, const void **fn_out,
+                              int *per_sm_out) {
   const void *fn = nullptr;
 #define RAK_PICK(M, O, U, B)                                                          \
   if (mode == M && off64 == (sizeof(O) == 8) && unit == U && batch == B)             \
@@ -887,10 +892,10 @@ cudaError_t resolve_lpa_slots(int mode, bool off64, bool unit, bool batch, const
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   static std::mutex mu;
-  static std::map<std::pair<const void *, int>, int> cache;
+  static std::map<std::pair<const void *, int>, int> cache;   // (kernel, device * 2 + stage)
   {
     std::lock_guard<std::mutex> lk(mu);
-    const auto it = cache.find({fn, dev});
+    const auto it = cache.find({fn, dev * 2 + (stage ? 1 : 0)});
     if (it != cache.end()) {
       *fn_out = fn;
       *per_sm_out = it->second;
@@ -898,13 +903,13 @@ cudaError_t resolve_lpa_slots(int mode, bool off64, bool unit, bool batch, const
     }
   }
   int per_sm = 0;
-  const size_t dyn = lpa_dynamic_smem(mode, unit);
+  const size_t dyn = lpa_dynamic_smem(mode, unit, stage);
   if (dyn > 0 && (e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn))) != cudaSuccess)
     return e;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, dyn)) != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   std::lock_guard<std::mutex> lk(mu);
-  cache[{fn, dev}] = per_sm;
+  cache[{fn, dev * 2 + (stage ? 1 : 0)}] = per_sm;
   *fn_out = fn;
   *per_sm_out = per_sm;
   return cudaSuccess;
@@ -914,7 +919,7 @@ template <int S>
 cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, bool batch, cudaStream_t st, int *grid_out) {
   const void *fn = nullptr;
   int per_sm = 0, dev = 0, sms = 0;
-  cudaError_t e = resolve_lpa_slots<S>(mode, off64, a.wt == nullptr, batch, &fn, &per_sm);
+  cudaError_t e = resolve_lpa_slots<S>(mode, off64, a.wt == nullptr, batch, a.stage != 0, &fn, &per_sm);
   if (e != cudaSuccess) return e;
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
@@ -930,7 +935,7 @@ cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, bool batch,
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(unsigned(grid));
   cfg.blockDim = dim3(256);
-  cfg.dynamicSmemBytes = lpa_dynamic_smem(mode, a.wt == nullptr);
+  cfg.dynamicSmemBytes = lpa_dynamic_smem(mode, a.wt == nullptr, a.stage != 0);
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;

@@ -3,5 +3,5 @@
 
 namespace rak {
 template cudaError_t launch_lpa_slots<16>(const LpaArgs &, int, bool, bool, cudaStream_t, int *);
-template cudaError_t resolve_lpa_slots<16>(int, bool, bool, bool, const void **, int *);
+template cudaError_t resolve_lpa_slots<16>(int, bool, bool, bool, bool, const void **, int *);
 }

@@ -268,7 +268,8 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   NA_TRY(cudaMemsetAsync(stats, 0, size_t(it_slots) * STATS_STRIDE * 8, st));
   NA_TRY(cudaMemsetAsync(rs, 0, sizeof(RunStateHost), st));
   // the kernel's code is loaded (CUDA loads modules lazily) before the timed part
-  if (iters > 0) NA_TRY(prepare_lpa(slots, mode, off64, g->weights == nullptr, false));
+  const bool stage = (o->edge_staging <= 0 ? DEFAULT_EDGE_STAGING : o->edge_staging) == 1;
+  if (iters > 0) NA_TRY(prepare_lpa(slots, mode, off64, g->weights == nullptr, false, stage));
   const auto t1 = std::chrono::steady_clock::now();
   if (ref_labels) NA_TRY(launch_init_mapped(membership, q, ref_pos, n, st));
   else NA_TRY(launch_init(membership, vcom1, q, n, st));
@@ -290,7 +291,7 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   // ties as in rak_lowmem_cuda: hashed during the first iterations of asynchronous runs
   const int tie = o->tie_break <= 0 ? (mode == RAK_MODE_ASYNC && !a.gpu_rule ? 2 : 1) : o->tie_break;
   a.tie_until = tie == 2 ? (o->tie_iterations > 0 ? o->tie_iterations : DEFAULT_TIE_ITERATIONS) : 0;
-  a.stage = (o->edge_staging <= 0 ? DEFAULT_EDGE_STAGING : o->edge_staging) == 1;
+  a.stage = stage;
   a.timeout_ns = o->wait_timeout_ns > 0 ? (long long)o->wait_timeout_ns : DEFAULT_WAIT_TIMEOUT_NS;
   if (iters > 0) {
     int grid = 0;

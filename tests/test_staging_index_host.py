@@ -5,7 +5,7 @@ read must fall inside the tile (offsets 0..STG_TILE-1) and hold a copied edge; e
 fall inside [eb, ee); every bulk copy must start and end on 16-byte boundaries inside [eb, ee)."""
 import pytest
 
-STG_TILE, B = 512, 4
+STG_TILE, B = 256, 4
 
 
 def walk(eb, ee, base_mis):
@@ -58,7 +58,7 @@ def walk(eb, ee, base_mis):
 
 @pytest.mark.parametrize("mis", [0, 1, 2, 3])
 def test_every_edge_once_in_order_and_in_bounds(mis):
-    lengths = list(range(0, 70)) + [511, 512, 513, 515, 516, 1023, 1024, 1025, 1027, 1500, 2048, 2051, 4099, 8192]
+    lengths = list(range(0, 70)) + [255, 256, 257, 259, 260, 511, 512, 513, 515, 516, 1023, 1024, 1025, 1027, 1500, 2048, 2051, 4099, 8192]
     for eb in (0, 1, 2, 3, 5, 1000, 1001, 4097):
         for n in lengths:
             ee = eb + n
