@@ -433,14 +433,45 @@ def batched_leg(ctx, count, steps, threads, stream, world=1, rank=0, dist=None):
                          "the slowest rank's" if world > 1 else "single GPU")}
 
 
-def serving_leg(ctx, rates, seconds, threads, seed=11):
+def my_requests(count, world, rank):
+    """Request i of a stream goes to rank i mod world (independent requests: no collective on the
+    data path; every rank draws the same arrival stream and submits its share at its times)."""
+    return [i for i in range(count) if i % world == rank]
+
+
+def gather_objects(dist, obj):
+    """Every rank's obj, in rank order (all_gather_object); without a process group, [obj]."""
+    if dist is None:
+        return [obj]
+    out = [None] * dist.get_world_size()
+    dist.all_gather_object(out, obj)
+    return out
+
+
+def merge_serving(parts):
+    """Merges per-rank serving results: latency percentiles over every request served by any rank;
+    the span is the slowest rank's (first submission to last result); counts are summed."""
+    lat = np.concatenate([np.asarray(p["lat"], np.float64) for p in parts]) if parts else np.zeros(0)
+    queued = np.concatenate([np.asarray(p["queued"], np.float64) for p in parts]) if parts else np.zeros(0)
+    span = max(p["span"] for p in parts)
+    requests = sum(len(p["lat"]) for p in parts)
+    edges = sum(p["edges"] for p in parts)
+    return {"requests": requests, "span_s": span, "graphs_per_s": requests / span, "edges_per_s": edges / span,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "queue_p50_ms": float(np.percentile(queued, 50)), "queue_p99_ms": float(np.percentile(queued, 99)),
+            "ranks": len(parts)}
+
+
+def serving_leg(ctx, rates, seconds, threads, seed=11, world=1, rank=0, dist=None):
     """Serving loop (rak_server_*) under Poisson arrivals: 98% of requests draw a graph from a pool
     of 64 graphs of the batched-launch mix, 2% are a symmetric R-MAT scale 22 / edge factor 16.
     Two arms per rate: "arena" -- every graph kept in device memory and submitted as a device CSR
     (packed by a device-to-device gather) -- and "host" -- page-locked host graphs uploaded per
     request. Latency is submit-to-result per request (measured by the server); graphs/s and edges/s
     over the span from the first submission to the last result. Quality: the modularity of each
-    served result against the same graph run alone through rak_lowmem_cuda."""
+    served result against the same graph run alone through rak_lowmem_cuda. With several ranks
+    (one GPU each) requests are dealt round-robin (my_requests) and the per-rank results are merged
+    on the host (merge_serving)."""
     import threading
     import torch
     import rak_lowmem as rl
@@ -501,23 +532,26 @@ def serving_leg(ctx, rates, seconds, threads, seed=11):
                                else srv.submit(graphs[k])) for k in ks]:
                         srv.wait(t, timeout=600.0)
                 st0 = srv.stats()
-                tickets = [None] * count
-                lat, queued, done_at, labels = [], [], [0.0] * count, {}
+                mine = my_requests(count, world, rank)
+                tickets = {}
+                lat, queued, done_at, labels = [], [], [], {}
                 ready = threading.Semaphore(0)
 
                 def waiter():
-                    for i in range(count):
+                    for i in mine:
                         ready.acquire()
                         lab, res = srv.wait(tickets[i], timeout=600.0)
-                        done_at[i] = time.perf_counter()
+                        done_at.append(time.perf_counter())
                         lat.append(res.time_ms)
                         queued.append(res.plan_ms)
                         labels.setdefault(int(picks[i]), lab)
 
                 th = threading.Thread(target=waiter)
                 th.start()
+                if dist is not None:
+                    dist.barrier()
                 start = time.perf_counter()
-                for i in range(count):
+                for i in mine:
                     due = start + arrivals[i]
                     while True:
                         d = due - time.perf_counter()
@@ -530,23 +564,32 @@ def serving_leg(ctx, rates, seconds, threads, seed=11):
                                   else srv.submit(graphs[k]))
                     ready.release()
                 th.join()
-                span = max(done_at) - start
+                span = max(done_at) - start if done_at else 0.0
                 st = srv.stats()
                 srv.close()
-                served = quality({k: ctx.modularity(graphs[k], lab) for k, lab in labels.items()})
-                edges = int(sum(graphs[int(k)].m for k in picks))
-                arms[f"{arm}_{rate}"] = {
-                    "arm": arm, "rate_req_s": rate, "requests": count, "large_requests": int(np.sum(picks == len(pool))),
-                    "graphs_per_s": count / span, "edges_per_s": edges / span, "offered_s": float(arrivals[-1]),
-                    "span_s": span, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                    "queue_p50_ms": float(np.percentile(queued, 50)), "queue_p99_ms": float(np.percentile(queued, 99)),
+                part = {"lat": lat, "queued": queued, "span": span,
+                        "edges": int(sum(graphs[int(picks[i])].m for i in mine)),
+                        "q": {k: ctx.modularity(graphs[k], lab) for k, lab in labels.items()}}
+                parts = gather_objects(dist, part)
+                merged = merge_serving(parts)
+                q_served = {}
+                for p_ in parts:
+                    for k, v in p_["q"].items():
+                        q_served.setdefault(k, v)
+                served = quality(q_served)
+                arms[f"{arm}_{rate}"] = dict(merged, **{
+                    "arm": arm, "rate_req_s": rate, "large_requests": int(np.sum(picks == len(pool))),
+                    "offered_s": float(arrivals[-1]),
+                    "sharding": (f"requests dealt round-robin to {world} ranks, results merged on the host"
+                                 if world > 1 else "single GPU"),
                     "launches": int(st["launches"] - st0["launches"]),
-                    "graphs_per_launch": count / max(1, st["launches"] - st0["launches"]),
+                    "graphs_per_launch": len(mine) / max(1, st["launches"] - st0["launches"]),
                     "max_concurrent_launches": int(st["max_concurrent_launches"]),
                     "load_ms_per_launch": (st["load_ms"] - st0["load_ms"]) / max(1, st["launches"] - st0["launches"]),
                     "run_ms_per_launch": (st["run_ms"] - st0["run_ms"]) / max(1, st["launches"] - st0["launches"]),
-                    "modularity": served}
-                log(f"[serving] {arm} {rate} req/s: {arms[f'{arm}_{rate}']}")
+                    "modularity": served})
+                if rank == 0:
+                    log(f"[serving] {arm} {rate} req/s: {arms[f'{arm}_{rate}']}")
     finally:
         for a in registered:
             cudart.cudaHostUnregister(a.ctypes.data)
@@ -723,8 +766,9 @@ def main():
     if args.batch_graphs > 0:
         batched = batched_leg(ctx, args.batch_graphs, 3, threads, stream, world, rank, pg)
     serving = None
-    if args.serving_seconds > 0 and world == 1:
-        serving = serving_leg(ctx, [int(x) for x in args.serving_rates.split(",")], args.serving_seconds, threads)
+    if args.serving_seconds > 0:
+        serving = serving_leg(ctx, [int(x) for x in args.serving_rates.split(",")], args.serving_seconds, threads,
+                              world=world, rank=rank, dist=pg)
 
     if rank == 0:
         last = results[-1]

@@ -76,3 +76,48 @@ def test_batch_mix_shares_are_the_full_mix():
             f = full[2 * j + rank]
             np.testing.assert_array_equal(g.offsets, f.offsets)
             np.testing.assert_array_equal(g.targets, f.targets)
+
+
+def _serving_rank(rank, world, port, out):
+    import datetime
+    import numpy as np
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        mine = bench.my_requests(101, world, rank)
+        rng = np.random.default_rng(rank)
+        part = {"lat": list(rng.random(len(mine)) * (rank + 1)), "queued": [0.5] * len(mine),
+                "span": 1.0 + rank, "edges": 10 * len(mine), "q": {rank: 0.5 + rank}}
+        parts = bench.gather_objects(dist, part)
+        out.put((rank, mine, parts, bench.merge_serving(parts)))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_serving_requests_dealt_and_merged_two_ranks():
+    """Serving sharded by request: ranks take disjoint shares that cover the stream, every rank
+    receives every rank's results, and the merge takes percentiles over all requests, the slowest
+    rank's span and summed counts."""
+    import numpy as np
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_serving_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    got = sorted((out.get(timeout=5) for _ in range(2)), key=lambda x: x[0])
+    shares = [set(m) for _, m, _, _ in got]
+    assert shares[0].isdisjoint(shares[1]) and shares[0] | shares[1] == set(range(101))
+    parts0, merged0 = got[0][2], got[0][3]
+    assert [len(p["lat"]) for p in parts0] == [51, 50] and merged0 == got[1][3]
+    lat = np.concatenate([p["lat"] for p in parts0])
+    assert merged0["requests"] == 101 and merged0["span_s"] == 2.0 and merged0["ranks"] == 2
+    assert merged0["p99_ms"] == pytest.approx(float(np.percentile(lat, 99)))
+    assert merged0["graphs_per_s"] == pytest.approx(101 / 2.0) and merged0["edges_per_s"] == pytest.approx(1010 / 2.0)

@@ -9,9 +9,10 @@ both land in one giant community), and prints both runs (time, iterations, trave
 for the record.
 The graphs are R-MAT scale RAK_REF_SCALE (default 18, edge factor 16, unit weights), a planted
 partition SBM and a road-like lattice (4-neighbour grid, 5% of edges deleted, 1% shortcuts). On the
-lattice the reference's νMG8 ends 5-7% higher (0.628 vs 0.585 at 2^25 vertices; neither the work
-order, the number of vertices in flight nor the reference's GPU sketch rules close it), so there
-the bound is 10% and the gap is printed; `RAK_REF_SCALE=24 RAK_REF_EF=32 RAK_REF_WEIGHTED=1 pytest tests/test_reference_gpu.py
+lattice most choices are ties between equally weighted labels; the asynchronous default breaks them
+by hash in its first iterations (rak_options.tie_break 2) and ends above the reference (0.687 vs
+0.628 at 2^25 vertices), where the reference's rule -- the most recently inserted key -- made it end
+5.8% below. `RAK_REF_SCALE=24 RAK_REF_EF=32 RAK_REF_WEIGHTED=1 pytest tests/test_reference_gpu.py
 -m gpu -s` runs the benchmark graph.
 """
 import json
@@ -65,7 +66,7 @@ def test_against_reference_gpu(ctx, slots):
                "speedup_time": info["time_ms"] / res.time_ms}
         print("REFGPU " + json.dumps(rec))
         assert lab.max() < g.n
-        tol = 0.10 if name.startswith("lattice") else 0.005 if slots > 1 else 0.05
+        tol = 0.005 if slots > 1 else 0.05
         # plus 1e-3 absolute: on unpermuted R-MAT both implementations can end in one giant
         # community (Q ~ 1e-5), where a relative tolerance compares noise
         assert q >= q_ref - tol * abs(q_ref) - 1e-3, rec
