@@ -122,7 +122,9 @@ typedef struct rak_options {
                                  warp scans read their edges from shared-memory tiles filled by bulk
                                  copies (TMA, cp.async.bulk); 2: every lane loads its edges from
                                  global memory. Results are the same either way. [2] */
-  int32_t reserved_i;
+  int32_t max_blocks;         /* 0: as many thread blocks as fit on the device; k > 0: the persistent
+                                 launch uses at most k blocks of 256 threads (fewer vertices in
+                                 flight at once; leaves SMs to other work) [0] */
   int64_t reserved[4];
 } rak_options;
 

@@ -226,6 +226,7 @@ struct Resolved {
   long long timeout_ns;  // bound on each device-side wait
   int tie_until;         // iterations with hashed Misra-Gries ties
   int stage;             // edge staging through shared memory
+  int max_blocks;        // cap on the persistent launch's blocks (0: none)
   Layout ly;
 };
 
@@ -280,6 +281,8 @@ rak_status resolve(rak_ctx *ctx, const rak_options *o, Resolved *r) {
   const int stg = o->edge_staging <= 0 ? rak::DEFAULT_EDGE_STAGING : o->edge_staging;
   if (stg != 1 && stg != 2) { set_err(ctx, "edge_staging must be -1, 0, 1 or 2"); return RAK_ERR_INVALID_ARGUMENT; }
   r->stage = stg == 1;
+  if (o->max_blocks < 0) { set_err(ctx, "max_blocks must be >= 0"); return RAK_ERR_INVALID_ARGUMENT; }
+  r->max_blocks = o->max_blocks;
   r->timeout_ns = o->wait_timeout_ns > 0 ? (long long)o->wait_timeout_ns : rak::DEFAULT_WAIT_TIMEOUT_NS;
   r->start = o->start_iteration;
   r->validate = o->validate;
@@ -535,7 +538,7 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
   a.sk_keys = b.skk.as<uint32_t>(); a.sk_wts = b.skw.as<float>();
   a.stats = b.stats.as<unsigned long long>(); a.rs = b.rs.p;
   a.iters = r.iters; a.start_iter = r.start; a.tolerance = r.tol; a.pickless_step = r.pickless;
-  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until; a.stage = r.stage;
+  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until; a.stage = r.stage; a.grid_cap = r.max_blocks;
 
   // the kernel's module is loaded here, not inside the timed region
   if (r.iters > 0) RAK_TRY(ctx, rak::prepare_lpa(r.slots, r.mode, gr->off64, gr->wt == nullptr, false, r.stage));
@@ -868,7 +871,7 @@ rak_status rak_graph_step(rak_ctx *ctx, rak_graph *gr, const rak_options *o, int
   a.sk_keys = b.skk.as<uint32_t>(); a.sk_wts = b.skw.as<float>();
   a.stats = b.stats.as<unsigned long long>(); a.rs = b.rs.p;
   a.iters = 1; a.start_iter = iteration; a.tolerance = r.tol; a.pickless_step = r.pickless;
-  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until; a.stage = r.stage;
+  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until; a.stage = r.stage; a.grid_cap = r.max_blocks;
   int grid = 0;
   RAK_TRY(ctx, rak::launch_lpa(a, r.slots, r.mode, gr->off64, st, &grid));
   unsigned long long s[rak::STATS_STRIDE] = {};
@@ -1175,7 +1178,7 @@ rak_status batch_enqueue(rak_ctx *ctx, rak_batch *b, const uint32_t *q, const Re
     a.stats = rb.stats.as<unsigned long long>(); a.rs = rb.rs.p;
     a.gid = b->gid.as<uint32_t>(); a.vbase = b->vbase.as<int64_t>(); a.gdone = b->gdone.as<uint8_t>();
     a.giters = b->giters.as<int32_t>(); a.gchanged = b->gchanged.as<unsigned long long>();
-    a.running = b->running.as<unsigned int>(); a.ngraphs = G; a.grid_cap = grid_cap;
+    a.running = b->running.as<unsigned int>(); a.ngraphs = G; a.grid_cap = grid_cap > 0 ? grid_cap : r.max_blocks;
     a.iters = r.iters; a.start_iter = r.start; a.tolerance = r.tol; a.pickless_step = r.pickless;
     a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until; a.stage = r.stage;
     int grid = 0;

@@ -727,11 +727,18 @@ __global__ void __launch_bounds__(256, RAK_MIN_BLOCKS) lpa_run(const LpaArgs a) 
     sc.w = UNIT ? nullptr : reinterpret_cast<float *>(lpa_dsm + tbytes) + size_t(w) * STG_STAGES * STG_TILE;
     sc.bar = smem_u32(lpa_dsm + tbytes * (UNIT ? 1 : 2)) + 8u * uint32_t(w * STG_STAGES);
     sc.phase = 0;
+    // the tiles and their mbarriers exist only in launches given the dynamic shared memory for them
+    // (lpa_dynamic_smem); the launch's actual size is checked before any of it is touched
+    uint32_t dyn_bytes;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn_bytes));
+    const bool have = a.stage && dyn_bytes >= stage_bytes(UNIT);
     // targets and weights must share their 16-byte alignment (one copy range serves both)
-    sc.on = a.stage && (UNIT || ((reinterpret_cast<uintptr_t>(a.tgt) ^ reinterpret_cast<uintptr_t>(a.wt)) & 15u) == 0);
-    if (lane < STG_STAGES) mbar_init(sc.bar + 8u * uint32_t(lane), 1);
-    fence_mbar_init();
-    __syncwarp();
+    sc.on = have && (UNIT || ((reinterpret_cast<uintptr_t>(a.tgt) ^ reinterpret_cast<uintptr_t>(a.wt)) & 15u) == 0);
+    if (have) {
+      if (lane < STG_STAGES) mbar_init(sc.bar + 8u * uint32_t(lane), 1);
+      fence_mbar_init();
+      __syncwarp();
+    }
   }
   unsigned int epoch = 0;
   for (int it = 0; it < a.iters; ++it) {

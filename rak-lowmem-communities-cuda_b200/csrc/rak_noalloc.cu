@@ -292,6 +292,7 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   const int tie = o->tie_break <= 0 ? (mode == RAK_MODE_ASYNC && !a.gpu_rule ? 2 : 1) : o->tie_break;
   a.tie_until = tie == 2 ? (o->tie_iterations > 0 ? o->tie_iterations : DEFAULT_TIE_ITERATIONS) : 0;
   a.stage = stage;
+  a.grid_cap = o->max_blocks > 0 ? o->max_blocks : 0;
   a.timeout_ns = o->wait_timeout_ns > 0 ? (long long)o->wait_timeout_ns : DEFAULT_WAIT_TIMEOUT_NS;
   if (iters > 0) {
     int grid = 0;

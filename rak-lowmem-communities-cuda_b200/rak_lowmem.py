@@ -45,7 +45,7 @@ class rak_options(C.Structure):
                 ("compute_modularity", C.c_int32), ("start_iteration", C.c_int32),
                 ("initial_flags", C.c_void_p), ("sketch_rule", C.c_int32), ("label_order", C.c_int32),
                 ("wait_timeout_ns", C.c_int64), ("tie_break", C.c_int32), ("tie_iterations", C.c_int32),
-                ("edge_staging", C.c_int32), ("reserved_i", C.c_int32), ("reserved", C.c_int64 * 4)]
+                ("edge_staging", C.c_int32), ("max_blocks", C.c_int32), ("reserved", C.c_int64 * 4)]
 
 
 class rak_result(C.Structure):
