@@ -608,6 +608,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
+                    help="an extra rak_options field for the timed runs (e.g. edge_staging=1); repeatable")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
@@ -658,6 +660,9 @@ def main():
     rg = rl.ResidentGraph(ctx, dg.csr if dg is not None else g)
     membership = torch.empty(g.n, dtype=torch.int32, device="cuda")
     opts = dict(slots=args.slots)
+    for kv in args.option:
+        k, v = kv.split("=", 1)
+        opts[k] = float(v) if "." in v else int(v)
 
     for _ in range(args.warmup):
         rg.run(membership, **opts)
@@ -774,8 +779,9 @@ def main():
         last = results[-1]
         cfg = describe(args.workload, spec, g)
         method = {"slots": args.slots, "mode": "async (in-place, pickless every 8th iteration)",
-                  "rules": "reference CPU sketch rules (last free slot, clamped decrement, linear argmax)",
-                  "labels": "start at positions of the reference degree-partition order; returned as vertex ids",
+                  "rules": "reference CPU sketch rules (last free slot, clamped decrement, linear argmax); "
+                           "ties among equal maxima broken by hash in the first 2 iterations (tie_break 2)",
+                  "labels": "vertex ids", "options": opts,
                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                   "l2": f"inputs larger than L2: graph {graph_bytes(g, spec['off_bits']) / 1e9:.1f} GB vs 126 MB L2"}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -97,13 +97,12 @@ typedef struct rak_options {
                                  rules (first free slot, unclamped, tournament argmax, move if
                                  w != 0, Boyer-Moore from the own label). SYNC runs 1 only;
                                  ASYNC and SYNC_SPLIT run either [1] */
-  int32_t label_order;        /* -1 or 0: mode default; 1: labels are vertex ids; 2: labels are
+  int32_t label_order;        /* -1 or 0: default [1]; 1: labels are vertex ids; 2: labels are
                                  positions in the reference GPU path's vertex order (degree
                                  partition, inc/rakLowmemCuda.hxx:505-519, 563), which its pickless
                                  rule compares; results are vertex ids either way; in a batch,
-                                 each graph's own order. Single-graph ASYNC runs: 2 [2]; batches
-                                 and the server: 1 [1], 2 on request; SYNC modes: 1 only. Graph
-                                 steps label by id and refuse 2 */
+                                 each graph's own order. ASYNC runs, batches and the server take
+                                 either; SYNC modes and graph steps label by id and refuse 2 */
   int64_t wait_timeout_ns;    /* 0: default [20 s]; bound on each device-side wait (the grid barrier
                                  between iterations). When it runs out the launch records
                                  RAK_ERR_TIMEOUT, every block leaves, and the call returns that
@@ -117,7 +116,7 @@ typedef struct rak_options {
                                  key with the largest hash of (vertex, key, l) (SplitMix64), then
                                  the reference's rule. CPU sketch rules only. ASYNC: 2 [2]; SYNC
                                  and SYNC_SPLIT: 1 [1], 2 on request (deterministic) */
-  int32_t tie_iterations;     /* 0: default [4]; iterations with hashed ties under tie_break 2 */
+  int32_t tie_iterations;     /* 0: default [2]; iterations with hashed ties under tie_break 2 */
   int32_t edge_staging;       /* -1 or 0: default; 1: vertices and split-vertex chunks that a whole
                                  warp scans read their edges from shared-memory tiles filled by bulk
                                  copies (TMA, cp.async.bulk); 2: every lane loads its edges from

@@ -58,7 +58,7 @@ constexpr int64_t DEFAULT_HUB_MIN = 65536;
 constexpr int64_t DEFAULT_HUB_CHUNK = 8192;
 constexpr int64_t MAX_LANE_MAX = 1024;
 // Iterations with hashed ties (rak_options.tie_break 2) when rak_options.tie_iterations is 0.
-constexpr int DEFAULT_TIE_ITERATIONS = 4;
+constexpr int DEFAULT_TIE_ITERATIONS = 2;
 // Edge staging (rak_options.edge_staging) when the option is 0: 1 on, 2 off.
 constexpr int DEFAULT_EDGE_STAGING = 2;
 // Bound on each device-side wait when rak_options.wait_timeout_ns is 0.

@@ -6,8 +6,8 @@
 // of asynchronous runs, lane_max, hub_min, hub_chunk, slots) is swept with the others held at the
 // best values so far, and the fastest candidate whose quality passes is kept. The label order
 // goes first: it changes how fast the asynchronous iteration settles the most (R-MAT, whose hubs
-// have small ids, settles sooner with id labels; grid-numbered graphs stall with them and fail the
-// quality gate). Objective: time to result (a run to convergence,
+// have small ids, settles sooner with id labels; under the reference's tie rule grid-numbered
+// graphs stall with them and fail the quality gate). Objective: time to result (a run to convergence,
 // best of `repeats`), since the layout also changes how fast the asynchronous iteration settles.
 // Quality gate: FP64 modularity (mean over graphs for a batch) at least
 // Q_start * (1 - quality_rel) - quality_abs, where Q_start is that of the caller's options.
@@ -166,7 +166,7 @@ rak_status rak_graph_autotune(rak_ctx *ctx, rak_graph *gr, const rak_options *ba
     }
     return m;
   };
-  return search(space, base, 2, run, best, log, log_cap, log_len);
+  return search(space, base, 1, run, best, log, log_cap, log_len);
 }
 
 rak_status rak_batch_autotune(rak_ctx *ctx, rak_batch *b, int64_t graphs, const rak_options *base,

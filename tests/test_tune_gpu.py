@@ -58,16 +58,22 @@ def test_batch_autotune():
 
 
 def test_label_order_is_tuned_under_the_quality_gate():
-    """Both label orders are tried first; on a grid-numbered lattice id labels stall (the pickless
-    rule blocks the first moves) and fail the gate, so the reference order is kept."""
+    """Both label orders are tried first. Under the reference's tie rule (tie_break 1) id labels
+    stall on a grid-numbered lattice (the pickless rule blocks the first moves) and fail the gate,
+    so the reference order is kept; with the default hashed ties both orders pass."""
     import torch
     g = rl.gen_lattice(512, 512, 0.05, 0.01, seed=7)
     sp = rl.tune_space(repeats=1, lane_max=[256], hub_min=[65536], hub_chunk=[8192], slots=[8])
     with rl.Context(0) as ctx:
         rg = rl.ResidentGraph(ctx, g)
         mem = torch.empty(g.n, dtype=torch.int32, device="cuda")
-        best, log = rg.autotune(mem, space=sp)
+        best, log = rg.autotune(mem, space=sp, label_order=2, tie_break=1)
         check_log(best, log, sp)
         assert log[0]["label_order"] == 2 and log[1]["label_order"] == 1
         assert log[1]["accepted"] == 0 and best["label_order"] == 2
+        best, log = rg.autotune(mem, space=sp)
+        check_log(best, log, sp)
+        assert log[0]["label_order"] == 1 and log[1]["label_order"] == 2
+        assert log[0]["accepted"] == 1 and log[1]["accepted"] == 1
+        assert log[0]["modularity"] > 0.5
         rg.close()
