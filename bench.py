@@ -44,6 +44,8 @@ WORKLOADS = {
     "rmat20_ef32_w": dict(kind="rmat", scale=20, ef=32, w=(1.0, 10.0), off_bits=32),
     # scale-16 graph of the reference's CPU-runnable case (unit weights)
     "rmat16_ef16": dict(kind="rmat", scale=16, ef=16, w=(1.0, 1.0), off_bits=32),
+    # a sparse graph whose labels (134 MB) exceed L2 but whose edges are few: DRAM-counter captures
+    "rmat25_ef4": dict(kind="rmat", scale=25, ef=4, w=(1.0, 1.0), off_bits=64),
     # largest single graph: scale 27 / ef 16 / unit weights / int64 offsets
     "rmat27_ef16": dict(kind="rmat", scale=27, ef=16, w=(1.0, 1.0), off_bits=64),
     # road-like lattice with 2^25 vertices (degree-regime graph 2)
