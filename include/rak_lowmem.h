@@ -97,7 +97,8 @@ typedef struct rak_options {
                                  rules (first free slot, unclamped, tournament argmax, move if
                                  w != 0, Boyer-Moore from the own label). SYNC runs 1 only;
                                  ASYNC and SYNC_SPLIT run either [1] */
-  int32_t label_order;        /* -1 or 0: default [1]; 1: labels are vertex ids; 2: labels are
+  int32_t label_order;        /* -1 or 0: default [1; 2 for ASYNC runs of one graph with slots 1
+                                 or 2]; 1: labels are vertex ids; 2: labels are
                                  positions in the reference GPU path's vertex order (degree
                                  partition, inc/rakLowmemCuda.hxx:505-519, 563), which its pickless
                                  rule compares; results are vertex ids either way; in a batch,

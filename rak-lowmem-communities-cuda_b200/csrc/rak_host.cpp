@@ -261,10 +261,12 @@ rak_status resolve(rak_ctx *ctx, const rak_options *o, Resolved *r) {
     set_err(ctx, "RAK_MODE_SYNC runs the CPU sketch rules (bit-exact with the reference CPU code)");
     return RAK_ERR_UNSUPPORTED;
   }
-  // labels by vertex id by default in every mode: with hashed ties (tie_break 2) id labels no longer
-  // stall on grid-numbered graphs, and on R-MAT they were faster and never collapsed in repeated
-  // runs where the reference order collapsed in some; the reference order stays one option away
-  r->order = o->label_order <= 0 ? 1 : o->label_order;
+  // labels by vertex id by default (rak::default_label_order): with hashed ties (tie_break 2) id
+  // labels no longer stall Misra-Gries runs on grid-numbered graphs, and on R-MAT they were faster
+  // and never collapsed in repeated runs where the reference order collapsed in some; asynchronous
+  // runs with one or two slots, whose sketches end on the last neighbour rather than on a tie, keep
+  // the reference order against the stall
+  r->order = o->label_order <= 0 ? rak::default_label_order(r->mode, r->slots) : o->label_order;
   if (r->order != 1 && r->order != 2) { set_err(ctx, "label_order must be -1, 0, 1 or 2"); return RAK_ERR_INVALID_ARGUMENT; }
   if (r->order == 2 && r->mode != RAK_MODE_ASYNC) {
     set_err(ctx, "the synchronous modes label vertices by id (bit-exact with the reference CPU code)");

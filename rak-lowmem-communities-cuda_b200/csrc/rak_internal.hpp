@@ -128,6 +128,15 @@ struct LpaArgs {
 
 enum Mode { MODE_ASYNC = 0, MODE_SYNC = 1, MODE_SPLIT = 2 };
 
+// Label order (rak_options.label_order) of single-graph runs when the option is 0: vertex ids (1),
+// except asynchronous runs with one or two slots, which take the reference GPU path's order (2).
+// Measured on B200: a sketch too small to hold a degree-4 neighbourhood (Boyer-Moore, MG2) ends on
+// the last neighbour it saw, on a grid-numbered graph the largest neighbour id, which the pickless
+// first iteration forbids, and with id labels the run stalls (lattice, Boyer-Moore: Q 0.003
+// against 0.607); larger Misra-Gries sketches hold the neighbourhood, break the tie by hash and are
+// faster on R-MAT with id labels. Synchronous modes always label by id.
+inline int default_label_order(int mode, int slots) { return mode == MODE_ASYNC && slots <= 2 ? 2 : 1; }
+
 // Per-iteration counters written by the LPA kernel.
 enum Stat { STAT_CHANGED = 0, STAT_EDGES = 1, STAT_PROCESSED = 2, STAT_HUBS_MOVED = 3, STAT_MOVED_EDGES = 4, STAT_WORK = 5 };
 constexpr int STATS_STRIDE = 8;

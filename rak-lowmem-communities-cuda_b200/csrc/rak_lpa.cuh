@@ -76,6 +76,28 @@ __device__ __forceinline__ float ld_weight(const float *p) {
 #endif
 }
 
+// Label gathers (neighbour labels, which change during the launch: plain coherent loads).
+// RAK_LABEL_HINT=1 gives them an L2 evict-last cache policy (an operand of the load instruction):
+// when the label array is larger than L2, the lines of frequently read labels then outlast the
+// streamed edge lines.
+#ifndef RAK_LABEL_HINT
+#define RAK_LABEL_HINT 0
+#endif
+__device__ __forceinline__ uint64_t l2_keep_policy() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint32_t ld_label(const uint32_t *p) {
+#if RAK_LABEL_HINT
+  uint32_t v;
+  asm volatile("ld.global.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(l2_keep_policy()) : "memory");
+  return v;
+#else
+  return *p;
+#endif
+}
+
 template <bool UNIT>
 __device__ __forceinline__ float edge_w(const float *wt, int64_t e) {
   if constexpr (UNIT) return 1.0f;
@@ -103,7 +125,7 @@ __device__ __forceinline__ void scan_range(Sketch<S> &sk, uint32_t u, int64_t e,
   while (e < ee) {
     uint32_t c[B];
 #pragma unroll
-    for (int j = 0; j < B; ++j) c[j] = vin[t[j]];
+    for (int j = 0; j < B; ++j) c[j] = ld_label(vin + t[j]);
     const int64_t en = e + int64_t(B) * st;
     uint32_t t2[B];
     float w2[B];
@@ -132,7 +154,7 @@ __device__ __forceinline__ void rescan_range(Sketch<S> &sk, uint32_t u, int64_t 
   for (; e < ee; ++e) {
     const uint32_t v = base + ld_edge(tgt + e);
     if (v == u) continue;
-    const uint32_t c = vin[v];
+    const uint32_t c = ld_label(vin + v);
     const float w = edge_w<UNIT>(wt, e);
 #pragma unroll
     for (int i = 0; i < S; ++i)
@@ -328,7 +350,7 @@ __device__ __forceinline__ void staged_scan(Sketch<S> &sk, StageCtx &sc, uint32_
           w[j] = UNIT ? 1.0f : bw[x];
         }
 #pragma unroll
-        for (int j = 0; j < B; ++j) c[j] = vin[t[j]];
+        for (int j = 0; j < B; ++j) c[j] = ld_label(vin + t[j]);
 #pragma unroll
         for (int j = 0; j < B; ++j)
           if (t[j] != u) sk_acc<S, RULE>(sk, c[j], w[j]);
@@ -358,7 +380,7 @@ __device__ __forceinline__ void staged_scan(Sketch<S> &sk, StageCtx &sc, uint32_
           }
         }
 #pragma unroll
-        for (int j = 0; j < B; ++j) c[j] = vin[t[j]];
+        for (int j = 0; j < B; ++j) c[j] = ld_label(vin + t[j]);
 #pragma unroll
         for (int j = 0; j < B; ++j)
           if (t[j] != u) sk_acc<S, RULE>(sk, c[j], w[j]);
@@ -392,7 +414,7 @@ __device__ __forceinline__ void exact_group_scan(Sketch<S> &sk, uint32_t u, int6
       if (e < ee) {
         const uint32_t v = base + ld_edge(tgt + e);
         w = edge_w<UNIT>(wt, e);
-        c = vin[v];
+        c = ld_label(vin + v);
         ok = v != u;
       }
       const int cnt = int(ee - e0 < G ? ee - e0 : G);

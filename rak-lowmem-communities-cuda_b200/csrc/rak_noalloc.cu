@@ -130,9 +130,10 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   if (rescan && !exact && slots > 1) return RAK_ERR_UNSUPPORTED;
   if (o->sketch_rule > 2 || o->label_order > 2) return RAK_ERR_INVALID_ARGUMENT;
   if (exact && o->sketch_rule == 2) return RAK_ERR_UNSUPPORTED;
-  // labels as in rak_lowmem_cuda: vertex ids by default; label_order 2 (asynchronous runs) takes
-  // positions in the reference GPU path's vertex order, two n-sized tables more in the array
-  const int order_kind = o->label_order <= 0 ? 1 : o->label_order;
+  // labels as in rak_lowmem_cuda: vertex ids by default (the reference GPU path's vertex order for
+  // asynchronous runs with one or two slots); label_order 2 (asynchronous runs) takes positions in that
+  // order, two n-sized tables more in the array
+  const int order_kind = o->label_order <= 0 ? default_label_order(mode, slots) : o->label_order;
   if (order_kind == 2 && sync) return RAK_ERR_UNSUPPORTED;
   const int iters = o->max_iterations;
   if (iters < 0 || iters > 1024 || !(o->tolerance >= 0) || o->wait_timeout_ns < 0) return RAK_ERR_INVALID_ARGUMENT;

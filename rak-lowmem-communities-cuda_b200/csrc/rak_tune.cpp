@@ -38,7 +38,9 @@ bool layout_ok(const rak_options &o) {
          o.hub_chunk <= o.hub_min;
 }
 
-rak_status search(const rak_tune_space *sp_in, const rak_options *base, int default_order, const Runner &run,
+// single_graph: a run whose options leave the label order at 0 takes rak::default_label_order
+// (by mode and slot count); batches label by vertex id.
+rak_status search(const rak_tune_space *sp_in, const rak_options *base, bool single_graph, const Runner &run,
                   rak_options *best, rak_tune_entry *log, int32_t log_cap, int32_t *log_len) {
   rak_tune_space sp;
   if (sp_in) sp = *sp_in;
@@ -55,7 +57,7 @@ rak_status search(const rak_tune_space *sp_in, const rak_options *base, int defa
   if (cur.lane_max == 0) cur.lane_max = int32_t(rak::DEFAULT_LANE_MAX);
   if (cur.hub_min == 0) cur.hub_min = int32_t(rak::DEFAULT_HUB_MIN);
   if (cur.hub_chunk == 0) cur.hub_chunk = int32_t(rak::DEFAULT_HUB_CHUNK);
-  if (cur.label_order <= 0) cur.label_order = cur.mode == RAK_MODE_ASYNC ? default_order : 1;
+  if (cur.label_order <= 0) cur.label_order = single_graph ? rak::default_label_order(cur.mode, cur.slots) : 1;
   int32_t n_log = 0;
   auto record = [&](const rak_options &o, const Measured &m, bool accepted) {
     if (log && n_log < log_cap) {
@@ -166,7 +168,7 @@ rak_status rak_graph_autotune(rak_ctx *ctx, rak_graph *gr, const rak_options *ba
     }
     return m;
   };
-  return search(space, base, 1, run, best, log, log_cap, log_len);
+  return search(space, base, true, run, best, log, log_cap, log_len);
 }
 
 rak_status rak_batch_autotune(rak_ctx *ctx, rak_batch *b, int64_t graphs, const rak_options *base,
@@ -201,7 +203,7 @@ rak_status rak_batch_autotune(rak_ctx *ctx, rak_batch *b, int64_t graphs, const 
     m.q = graphs > 0 ? sum / double(graphs) : 0;
     return m;
   };
-  return search(space, base, 1, run, best, log, log_cap, log_len);
+  return search(space, base, false, run, best, log, log_cap, log_len);
 }
 
 }  // extern "C"

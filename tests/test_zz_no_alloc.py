@@ -72,7 +72,7 @@ def test_noalloc_refuses_graphs_beyond_the_array():
 
 
 def test_noalloc_async_default_is_valid_and_matches_quality():
-    """The default asynchronous mode (reference label order, in-place updates) is not deterministic:
+    """The default asynchronous mode (id labels, in-place updates) is not deterministic:
     its labels must be valid vertex ids and its modularity close to the allocating entry point's."""
     import torch
     g = rl.gen_sbm(20000, 40, 12.0, 20.0, seed=26)
