@@ -40,6 +40,9 @@ __device__ __forceinline__ void sk_clear(Sketch<S> &s, uint32_t d = NONE) {
 // every slot keyed c; otherwise the LAST zero-weight slot takes (c, x); otherwise every weight
 // drops by x, clamped at zero. Only adds, subtracts and max: bit-identical to the CPU.
 // Hits (the common case once labels settle) leave early; the miss path runs only when needed.
+#ifndef RAK_MG_MINFIRST
+#define RAK_MG_MINFIRST 0
+#endif
 template <int S>
 __device__ __forceinline__ void mg_acc(Sketch<S> &s, uint32_t c, float x) {
   bool hit = false;
@@ -47,6 +50,17 @@ __device__ __forceinline__ void mg_acc(Sketch<S> &s, uint32_t c, float x) {
   for (int i = 0; i < S; ++i)
     if (s.k[i] == c) { s.w[i] = __fadd_rn(s.w[i], x); hit = true; }
   if (hit) return;
+#if RAK_MG_MINFIRST
+  // every weight positive: no free slot, the decrement follows (same outcome as the search below)
+  float mn = s.w[0];
+#pragma unroll
+  for (int i = 1; i < S; ++i) mn = fminf(mn, s.w[i]);
+  if (mn > 0.0f) {
+#pragma unroll
+    for (int i = 0; i < S; ++i) s.w[i] = fmaxf(__fsub_rn(s.w[i], x), 0.0f);
+    return;
+  }
+#endif
   int f = -1;
 #pragma unroll
   for (int i = 0; i < S; ++i)

@@ -543,7 +543,7 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
   a.sk_keys = b.skk.as<uint32_t>(); a.sk_wts = b.skw.as<float>();
   a.stats = b.stats.as<unsigned long long>(); a.rs = b.rs.p;
   a.iters = r.iters; a.start_iter = r.start; a.tolerance = r.tol; a.pickless_step = r.pickless;
-  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until; a.stage = r.stage; a.grid_cap = r.max_blocks;
+  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until; a.stage = r.stage; a.grid_cap = r.max_blocks;
 
   // the kernel's module is loaded here, not inside the timed region
   if (r.iters > 0) RAK_TRY(ctx, rak::prepare_lpa(r.slots, r.mode, gr->off64, gr->wt == nullptr, false, r.stage));
@@ -876,7 +876,7 @@ rak_status rak_graph_step(rak_ctx *ctx, rak_graph *gr, const rak_options *o, int
   a.sk_keys = b.skk.as<uint32_t>(); a.sk_wts = b.skw.as<float>();
   a.stats = b.stats.as<unsigned long long>(); a.rs = b.rs.p;
   a.iters = 1; a.start_iter = iteration; a.tolerance = r.tol; a.pickless_step = r.pickless;
-  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until; a.stage = r.stage; a.grid_cap = r.max_blocks;
+  a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until; a.stage = r.stage; a.grid_cap = r.max_blocks;
   int grid = 0;
   RAK_TRY(ctx, rak::launch_lpa(a, r.slots, r.mode, gr->off64, st, &grid));
   unsigned long long s[rak::STATS_STRIDE] = {};
@@ -1185,7 +1185,7 @@ rak_status batch_enqueue(rak_ctx *ctx, rak_batch *b, const uint32_t *q, const Re
     a.giters = b->giters.as<int32_t>(); a.gchanged = b->gchanged.as<unsigned long long>();
     a.running = b->running.as<unsigned int>(); a.ngraphs = G; a.grid_cap = grid_cap > 0 ? grid_cap : r.max_blocks;
     a.iters = r.iters; a.start_iter = r.start; a.tolerance = r.tol; a.pickless_step = r.pickless;
-    a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(r.slots, a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until; a.stage = r.stage;
+    a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for_batch(a.n, gr->m, G); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until; a.stage = r.stage;
     int grid = 0;
     RAK_TRY(ctx, rak::launch_lpa(a, r.slots, r.mode, true, st, &grid, true));
   }

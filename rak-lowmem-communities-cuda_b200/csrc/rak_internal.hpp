@@ -150,13 +150,19 @@ template <int S>
 cudaError_t launch_lpa_slots(const LpaArgs &a, int mode, bool off64, bool batch, cudaStream_t st, int *grid_out);
 template <int S>
 cudaError_t resolve_lpa_slots(int mode, bool off64, bool unit, bool batch, bool stage, const void **fn, int *per_sm);
-// Whether neighbour marking inside work items reads each flag before storing it. Measured to pay
-// for the Boyer-Moore sketch on graphs of 2^20 vertices and more whose average degree is 8 or more
-// (R-MAT s22-s24: 25-35% faster; SBM 4M: 5%), where many moved vertices mark the same hub flags,
-// and to cost otherwise (2D lattices of degree ~4: 23-30% slower; small graphs, whose flags stay
-// in L1).
-inline int mark_test_for(int slots, int64_t n, int64_t m) {
-  return slots == 1 && n >= (int64_t(1) << 20) && m >= 8 * n ? 1 : 0;
+// Whether neighbour marking reads each flag (through L1) before storing it. Measured on B200 with
+// the read through L1, test on / off, νMG8 and νBM: R-MAT scale 24 ef 32 (16.8 M vertices) 31.3 /
+// 36.9 ms and 23.1 / 32.2 ms; R-MAT scale 27 ef 16 (134 M) 128.0 / 135.6 ms and 125.6 / 139.5 ms --
+// many moved vertices mark the same flags, and a flag line in L1 answers without a request to L2.
+// On smaller or sparser graphs the read only lengthens each moved vertex's marking: SBM 2 M
+// vertices (degree 16) 1.43 / 1.33 ms, R-MAT scale 18 0.89 / 0.81 ms, SBM 100 k 0.83 / 0.32 ms,
+// 2D lattice 2^25 (degree ~4) 12.8 / 12.0 ms. Single graphs test from 2^22 vertices with average
+// degree 8 or more.
+inline int mark_test_for(int64_t n, int64_t m) { return n >= (int64_t(1) << 22) && m >= 8 * n ? 1 : 0; }
+// Batches (each graph's flags a compact range, its neighbours inside it): the single-graph rule at
+// the batch's mean graph size.
+inline int mark_test_for_batch(int64_t n, int64_t m, int64_t graphs) {
+  return graphs > 0 ? mark_test_for(n / graphs, m / graphs) : 0;
 }
 // Loads and resolves the kernel a run will launch (outside its timed region).
 cudaError_t prepare_lpa(int slots, int mode, bool off64, bool unit, bool batch, bool stage);

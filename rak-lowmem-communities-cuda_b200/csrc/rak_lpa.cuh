@@ -57,8 +57,17 @@ __device__ __forceinline__ uint64_t l2_stream_policy() {
   asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
   return p;
 }
+// RAK_L1_HINTS=1: edge-stream loads allocate in L1 as evict-first and label gathers as evict-last,
+// so the streamed edge lines leave L1 before the labels that neighbours share.
+#ifndef RAK_L1_HINTS
+#define RAK_L1_HINTS 0
+#endif
 __device__ __forceinline__ uint32_t ld_edge(const uint32_t *p) {
-#if RAK_STREAM_HINT
+#if RAK_L1_HINTS
+  uint32_t v;
+  asm("ld.global.nc.L1::evict_first.u32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+#elif RAK_STREAM_HINT
   uint32_t v;
   asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(l2_stream_policy()));
   return v;
@@ -67,7 +76,11 @@ __device__ __forceinline__ uint32_t ld_edge(const uint32_t *p) {
 #endif
 }
 __device__ __forceinline__ float ld_weight(const float *p) {
-#if RAK_STREAM_HINT
+#if RAK_L1_HINTS
+  float v;
+  asm("ld.global.nc.L1::evict_first.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+#elif RAK_STREAM_HINT
   float v;
   asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(l2_stream_policy()));
   return v;
@@ -79,7 +92,7 @@ __device__ __forceinline__ float ld_weight(const float *p) {
 // Label gathers (neighbour labels, which change during the launch: plain coherent loads).
 // RAK_LABEL_HINT=1 gives them an L2 evict-last cache policy (an operand of the load instruction):
 // when the label array is larger than L2, the lines of frequently read labels then outlast the
-// streamed edge lines.
+// streamed edge lines; RAK_LABEL_HINT=2 reads them from L2 only (not cached in L1).
 #ifndef RAK_LABEL_HINT
 #define RAK_LABEL_HINT 0
 #endif
@@ -89,10 +102,20 @@ __device__ __forceinline__ uint64_t l2_keep_policy() {
   return p;
 }
 __device__ __forceinline__ uint32_t ld_label(const uint32_t *p) {
-#if RAK_LABEL_HINT
+#if RAK_L1_HINTS && RAK_LABEL_HINT == 1
+  uint32_t v;
+  asm volatile("ld.global.L1::evict_last.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(l2_keep_policy()) : "memory");
+  return v;
+#elif RAK_L1_HINTS
+  uint32_t v;
+  asm volatile("ld.global.L1::evict_last.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+#elif RAK_LABEL_HINT == 1
   uint32_t v;
   asm volatile("ld.global.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(l2_keep_policy()) : "memory");
   return v;
+#elif RAK_LABEL_HINT == 2
+  return __ldcg(p);
 #else
   return *p;
 #endif
@@ -144,6 +167,116 @@ __device__ __forceinline__ void scan_range(Sketch<S> &sk, uint32_t u, int64_t e,
   }
 }
 
+// Neighbour marking reads a neighbour's flag before storing it when the launch asks for it
+// (LpaArgs::mark_test, mark_test_for). The read goes through L1: most neighbours of a moved vertex
+// are flagged already, and a flag line that L1 holds answers without a request to L2. In the
+// synchronous modes the flags being set are only set during an iteration (and L1 is invalidated
+// by the grid barrier's acquire), so a read can at worst miss a fresh mark and store it again. In
+// the asynchronous mode a line L1 holds can also show a flag that another SM has cleared since
+// (its vertex was processed); that neighbour is then not marked again for this move -- the same
+// kind of lost update as the mode's unordered plain stores, measured with no change of modularity
+// (R-MAT scale 24 and 27). RAK_MARK_FORCE=1/2 forces the test on/off (measurements).
+#ifndef RAK_MARK_FORCE
+#define RAK_MARK_FORCE 0
+#endif
+__device__ __forceinline__ uint32_t ld_flag_test(const uint8_t *p) { return *p; }
+
+// ---- one lane per vertex: the edge list read in 16-byte vectors -------------------------------
+//
+// A lane that scans its own vertex reads 4 targets (and 4 weights) per load instead of one: the
+// L1 looks up one sector per 4 edges instead of one per edge, and a warp issues a quarter of the
+// edge-stream loads. Requires targets (and weights) at 16-byte aligned addresses (checked per
+// launch, lane_vec_ok). Vector v covers edges 4v .. 4v+3; edges outside [e, ee) are masked with the
+// target u itself, which the self-loop rule skips, so the lane accumulates exactly edges e .. ee-1
+// in order, as scan_range with stride 1 does. Whole-vector loads stay inside [4*floor(e/4), ee);
+// the last vector of a range whose end is not a multiple of 4 is read edge by edge.
+template <bool UNIT>
+__device__ __forceinline__ void load_vec4(int64_t v, int64_t ee, const uint32_t *tgt, const float *wt, uint4 &t4,
+                                          float4 &w4) {
+  const int64_t x0 = v << 2;
+  if (x0 + 4 <= ee) {
+#if RAK_L1_HINTS
+    asm("ld.global.nc.L1::evict_first.v4.u32 {%0, %1, %2, %3}, [%4];"
+        : "=r"(t4.x), "=r"(t4.y), "=r"(t4.z), "=r"(t4.w) : "l"(tgt + x0));
+    if constexpr (!UNIT)
+      asm("ld.global.nc.L1::evict_first.v4.f32 {%0, %1, %2, %3}, [%4];"
+          : "=f"(w4.x), "=f"(w4.y), "=f"(w4.z), "=f"(w4.w) : "l"(wt + x0));
+#else
+    t4 = __ldg(reinterpret_cast<const uint4 *>(tgt) + v);
+    if constexpr (!UNIT) w4 = __ldg(reinterpret_cast<const float4 *>(wt) + v);
+#endif
+  } else {
+    t4.x = x0 < ee ? ld_edge(tgt + x0) : 0u;
+    t4.y = x0 + 1 < ee ? ld_edge(tgt + x0 + 1) : 0u;
+    t4.z = x0 + 2 < ee ? ld_edge(tgt + x0 + 2) : 0u;
+    t4.w = 0u;   // x0 + 3 >= ee here
+    if constexpr (!UNIT) {
+      w4.x = x0 < ee ? ld_weight(wt + x0) : 0.0f;
+      w4.y = x0 + 1 < ee ? ld_weight(wt + x0 + 1) : 0.0f;
+      w4.z = x0 + 2 < ee ? ld_weight(wt + x0 + 2) : 0.0f;
+      w4.w = 0.0f;
+    }
+  }
+}
+
+__device__ __forceinline__ bool lane_vec_ok(const uint32_t *tgt, const float *wt) {
+  return ((reinterpret_cast<uintptr_t>(tgt) | (wt ? reinterpret_cast<uintptr_t>(wt) : 0)) & 15u) == 0;
+}
+
+template <int S, bool UNIT, int RULE>
+__device__ __forceinline__ void scan_lane(Sketch<S> &sk, uint32_t u, int64_t e, int64_t ee, const uint32_t *tgt,
+                                          const float *wt, const uint32_t *vin, uint32_t base) {
+  if (e >= ee) return;
+  int64_t v = e >> 2;
+  const int64_t vend = (ee + 3) >> 2;
+  uint4 t4;
+  float4 w4 = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+  load_vec4<UNIT>(v, ee, tgt, wt, t4, w4);
+  for (; v < vend; ++v) {
+    const int64_t x0 = v << 2;
+    uint32_t t[4] = {t4.x, t4.y, t4.z, t4.w};
+    float w[4] = {w4.x, w4.y, w4.z, w4.w};
+    uint32_t c[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int64_t x = x0 + j;
+      t[j] = x >= e && x < ee ? base + t[j] : u;
+      c[j] = t[j] != u ? ld_label(vin + t[j]) : NONE;
+    }
+    if (v + 1 < vend) load_vec4<UNIT>(v + 1, ee, tgt, wt, t4, w4);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (t[j] != u) sk_acc<S, RULE>(sk, c[j], UNIT ? 1.0f : w[j]);
+  }
+}
+
+// Neighbour marking of a moved vertex scanned by one lane (mark_range with stride 1), from 16-byte
+// vectors of targets, two vectors in flight; TEST as in mark_range.
+template <bool TEST>
+__device__ __forceinline__ void mark_lane(uint32_t u, int64_t e, int64_t ee, const uint32_t *tgt, uint8_t *fout,
+                                          uint32_t base) {
+  if (e >= ee) return;
+  const int64_t vend = (ee + 3) >> 2;
+  float4 unused;
+  for (int64_t v = e >> 2; v < vend; v += 2) {
+    uint4 a4, b4 = make_uint4(0, 0, 0, 0);
+    load_vec4<true>(v, ee, tgt, nullptr, a4, unused);
+    if (v + 1 < vend) load_vec4<true>(v + 1, ee, tgt, nullptr, b4, unused);
+    uint32_t t[8] = {a4.x, a4.y, a4.z, a4.w, b4.x, b4.y, b4.z, b4.w};
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int64_t x = (v << 2) + j;
+      t[j] = x >= e && x < ee ? base + t[j] : u;
+    }
+    uint32_t f[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) f[j] = t[j] == u ? 1u : (TEST ? ld_flag_test(fout + t[j]) : 0u);
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (!f[j]) fout[t[j]] = 1;
+  }
+}
+
 // Exact weights of the sketch keys in edge order (inc/rakLowmem.hxx:154-162), one lane.
 template <int S, bool UNIT>
 __device__ __forceinline__ void rescan_range(Sketch<S> &sk, uint32_t u, int64_t e, int64_t ee,
@@ -166,14 +299,9 @@ __device__ __forceinline__ void rescan_range(Sketch<S> &sk, uint32_t u, int64_t 
 // Marks neighbours e, e+st, ... < ee of a moved vertex u as affected (inc/rakCuda.hxx:95-103),
 // except u itself (the reference CPU loop clears u after marking, inc/rakLowmem.hxx:203,209).
 // Pipelined in batches of eight: the next batch's targets load while this batch is stored.
-// test: store a flag only if it reads as clear (from L2, ld.cg, not a possibly stale L1 line). A
-// random byte store costs the L2 a partial write, about half the rate of a read, and most
-// neighbours of a moved vertex are flagged already; but the read adds a dependent round trip to
-// the marking of each vertex. Measured: testing pays in the split-vertex marking pass and for the
-// Boyer-Moore sketch on graphs of a million vertices and more (R-MAT scale 22-24: +15%), not
-// inside Misra-Gries items (-16%) nor on small graphs, whose flags stay in L1 (SBM 100k: 2.6x
-// slower). The Boyer-Moore kernels choose per launch (LpaArgs::mark_test); the Misra-Gries ones
-// never test inside items.
+// test: store a flag only if it reads as clear (ld_flag_test). A random byte store costs the L2 a
+// partial write, and most neighbours of a moved vertex are flagged already on large graphs; on
+// small or sparse ones the read only lengthens the marking (mark_test_for chooses per launch).
 template <bool TEST>
 __device__ __forceinline__ void mark_range(uint32_t u, int64_t e, int64_t ee, int st, const uint32_t *tgt,
                                            uint8_t *fout, uint32_t base) {
@@ -187,7 +315,7 @@ __device__ __forceinline__ void mark_range(uint32_t u, int64_t e, int64_t ee, in
   while (e < ee) {
     uint32_t f[MB];
 #pragma unroll
-    for (int j = 0; j < MB; ++j) f[j] = v[j] == u ? 1u : (TEST ? uint32_t(__ldcg(fout + v[j])) : 0u);
+    for (int j = 0; j < MB; ++j) f[j] = v[j] == u ? 1u : (TEST ? ld_flag_test(fout + v[j]) : 0u);
     const int64_t en = e + int64_t(MB) * st;
     uint32_t v2[MB];
 #pragma unroll
@@ -204,16 +332,16 @@ __device__ __forceinline__ void mark_range(uint32_t u, int64_t e, int64_t ee, in
   }
 }
 
-// Neighbour marking inside work items (see mark_range).
+
+template <int S>
+__device__ __forceinline__ bool mark_tested(const LpaArgs &a) {
+  return RAK_MARK_FORCE == 1 || (RAK_MARK_FORCE == 0 && a.mark_test != 0);
+}
 template <int S>
 __device__ __forceinline__ void mark_item(const LpaArgs &a, uint32_t u, int64_t e, int64_t ee, int st,
                                           const uint32_t *tgt, uint8_t *fout, uint32_t base) {
-  if constexpr (S == 1) {
-    if (a.mark_test) mark_range<true>(u, e, ee, st, tgt, fout, base);
-    else mark_range<false>(u, e, ee, st, tgt, fout, base);
-  } else {
-    mark_range<false>(u, e, ee, st, tgt, fout, base);
-  }
+  if (mark_tested<S>(a)) mark_range<true>(u, e, ee, st, tgt, fout, base);
+  else mark_range<false>(u, e, ee, st, tgt, fout, base);
 }
 
 // ---- edge tiles staged in shared memory by the bulk-copy engine (TMA) -------------------------
@@ -516,7 +644,9 @@ __device__ __forceinline__ void lane_batch(const LpaArgs &a, const G_<O> &g, con
   const int64_t eb = int64_t(__ldg(g.off + u)), ee = int64_t(__ldg(g.off + u + 1));
   Sketch<S> sk;
   sk_clear<S, RULE>(sk, d);
-  scan_range<S, UNIT, RULE>(sk, u, eb, ee, 1, g.tgt, g.wt, vin, base);
+  const bool vec = lane_vec_ok(g.tgt, g.wt);
+  if (vec) scan_lane<S, UNIT, RULE>(sk, u, eb, ee, g.tgt, g.wt, vin, base);
+  else scan_range<S, UNIT, RULE>(sk, u, eb, ee, 1, g.tgt, g.wt, vin, base);
   if constexpr (MODE == MODE_SYNC && S > 1)
     if (a.rescan) rescan_range<S, UNIT>(sk, u, eb, ee, g.tgt, g.wt, vin, base);
   uint32_t c;
@@ -535,7 +665,9 @@ __device__ __forceinline__ void lane_batch(const LpaArgs &a, const G_<O> &g, con
     cnt.changed += 1;
     cnt.moved_edges += (unsigned long long)(ee - eb);
     count_move<BATCH>(a, gi, it);
-    mark_item<S>(a, u, eb, ee, 1, g.tgt, fout, base);
+    if (!vec) mark_item<S>(a, u, eb, ee, 1, g.tgt, fout, base);
+    else if (mark_tested<S>(a)) mark_lane<true>(u, eb, ee, g.tgt, fout, base);
+    else mark_lane<false>(u, eb, ee, g.tgt, fout, base);
   }
 }
 

@@ -286,7 +286,7 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   a.pickless_step = o->pickless_step < 0 ? (mode == RAK_MODE_ASYNC ? 8 : 0) : o->pickless_step;
   a.check_on_pickless = o->check_on_pickless < 0 ? (mode == RAK_MODE_ASYNC ? 0 : 1) : (o->check_on_pickless ? 1 : 0);
   a.rescan = rescan;
-  a.mark_test = mark_test_for(slots, n, g->m);
+  a.mark_test = mark_test_for(n, g->m);
   // rule sets as in rak_lowmem_cuda: the CPU rules unless sketch_rule asks for the GPU ones
   a.gpu_rule = mode != RAK_MODE_SYNC && o->sketch_rule == 2;
   // ties as in rak_lowmem_cuda: hashed during the first iterations of asynchronous runs
