@@ -183,10 +183,9 @@ __device__ __forceinline__ uint32_t ld_flag_test(const uint8_t *p) { return *p; 
 
 // ---- one lane per vertex: the edge list read in 16-byte vectors -------------------------------
 //
-// A lane that scans its own vertex reads 4 targets (and 4 weights) per load instead of one: the
-// L1 looks up one sector per 4 edges instead of one per edge, and a warp issues a quarter of the
-// edge-stream loads. Requires targets (and weights) at 16-byte aligned addresses (checked per
-// launch, lane_vec_ok). Vector v covers edges 4v .. 4v+3; edges outside [e, ee) are masked with the
+// A lane that scans its own vertex of degree RAK_VEC_MIN_DEG or more reads 4 targets (and 4
+// weights) per load instead of one: a warp issues a quarter of the edge-stream loads. Requires
+// targets (and weights) at 16-byte aligned addresses (checked per launch, lane_vec_ok). Vector v covers edges 4v .. 4v+3; edges outside [e, ee) are masked with the
 // target u itself, which the self-loop rule skips, so the lane accumulates exactly edges e .. ee-1
 // in order, as scan_range with stride 1 does. Whole-vector loads stay inside [4*floor(e/4), ee);
 // the last vector of a range whose end is not a multiple of 4 is read edge by edge.
@@ -219,6 +218,14 @@ __device__ __forceinline__ void load_vec4(int64_t v, int64_t ee, const uint32_t 
   }
 }
 
+// Vector loads pay only on longer lists: a list's first and last vector carry masked positions,
+// and the short lists of sparse graphs are mostly such vectors. Measured on B200 (vectors from
+// degree 32 / always / never): 2D lattice 2^25 (degree ~4) 9.73 / 12.05 / 9.73 ms; R-MAT scale 25
+// ef 4 8.22 / 8.51 / 8.10 ms; R-MAT scale 27 ef 16 128.0 / 128.5 / 130.2 ms; R-MAT scale 24 ef 32
+// weighted 32.5 / 32.6 / 33.1 ms.
+#ifndef RAK_VEC_MIN_DEG
+#define RAK_VEC_MIN_DEG 32
+#endif
 __device__ __forceinline__ bool lane_vec_ok(const uint32_t *tgt, const float *wt) {
   return ((reinterpret_cast<uintptr_t>(tgt) | (wt ? reinterpret_cast<uintptr_t>(wt) : 0)) & 15u) == 0;
 }
@@ -644,7 +651,7 @@ __device__ __forceinline__ void lane_batch(const LpaArgs &a, const G_<O> &g, con
   const int64_t eb = int64_t(__ldg(g.off + u)), ee = int64_t(__ldg(g.off + u + 1));
   Sketch<S> sk;
   sk_clear<S, RULE>(sk, d);
-  const bool vec = lane_vec_ok(g.tgt, g.wt);
+  const bool vec = lane_vec_ok(g.tgt, g.wt) && ee - eb >= RAK_VEC_MIN_DEG;
   if (vec) scan_lane<S, UNIT, RULE>(sk, u, eb, ee, g.tgt, g.wt, vin, base);
   else scan_range<S, UNIT, RULE>(sk, u, eb, ee, 1, g.tgt, g.wt, vin, base);
   if constexpr (MODE == MODE_SYNC && S > 1)
