@@ -129,3 +129,39 @@ def test_edge_inputs_async_valid(ctx, slots):
         assert lab.max() < g.n and res.iterations >= 1
         q_oracle = orc.modularity(orc.Graph.of(g), lab)
         assert res.modularity == pytest.approx(q_oracle, rel=1e-9, abs=1e-12)
+
+
+def _device_csr_at(g, shift):
+    """g on the device with its targets (and weights) starting `shift` elements into a buffer, so
+    the arrays are 4-byte but not 16-byte aligned when shift % 4 != 0."""
+    import torch
+    off = torch.from_numpy(np.ascontiguousarray(g.offsets)).cuda()
+    tbuf = torch.zeros(g.m + shift, dtype=torch.int32, device="cuda")
+    tbuf[shift:] = torch.from_numpy(g.targets.view(np.int32)).cuda()
+    tgt = tbuf[shift:]
+    wt = None
+    if g.weights is not None:
+        wbuf = torch.zeros(g.m + shift, dtype=torch.float32, device="cuda")
+        wbuf[shift:] = torch.from_numpy(g.weights).cuda()
+        wt = wbuf[shift:]
+    return (off, tbuf, tgt, wt), rl.device_csr(off, tgt, wt)
+
+
+@pytest.mark.parametrize("shift", [0, 1, 3])
+@pytest.mark.parametrize("mode", [rl.MODE_SYNC, rl.MODE_SYNC_SPLIT])
+def test_unaligned_edge_arrays(ctx, shift, mode):
+    """One-lane vertices read their edge lists in 16-byte vectors when the target and weight arrays
+    are 16-byte aligned, and element by element otherwise: the labels are the oracle's either way
+    (weighted R-MAT, one-lane lists both shorter and longer than the vector threshold)."""
+    import torch
+    g = rl.gen_rmat(13, 16, seed=31, w_lo=1.0, w_hi=10.0)
+    keep, csr = _device_csr_at(g, shift)
+    assert (keep[2].data_ptr() % 16 == 0) == (shift % 4 == 0)
+    for slots in (8, 1):
+        o = orc.make_opts(slots=slots, rescan=1 if mode == rl.MODE_SYNC else 0,
+                          split=1 if mode == rl.MODE_SYNC_SPLIT else 0, layout=orc.DEFAULT_LAYOUT)
+        ref, it, edges = orc.sync_run(orc.Graph.of(g), o)
+        out = torch.empty(g.n, dtype=torch.int32, device="cuda")
+        res = ctx.lowmem_device(csr, out, mode=mode, slots=slots)
+        np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), ref)
+        assert res.iterations == it and res.traversed_edges == edges
