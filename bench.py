@@ -176,10 +176,12 @@ def traffic_for(workload):
 def algorithmic_bytes(res, off_bytes, weighted):
     """Bytes the LPA kernel must move (per run): for each processed vertex 12*deg (target, weight,
     neighbour label; 8*deg without weights) + offset pair + own label + flag read/write; for each
-    moved vertex its label write plus 5*deg to re-read targets and mark neighbour flags."""
+    moved vertex its label write, and for each moved vertex whose neighbours were marked (all but
+    the moves of dense iterations, rak_options.dense_pct) 5*deg to re-read targets and mark
+    neighbour flags."""
     per_edge = 12 if weighted else 8
     return (per_edge * res.traversed_edges + (off_bytes + 4 + 1 + 1) * res.processed_vertices
-            + 4 * res.moved_vertices + 5 * res.moved_edges)
+            + 4 * res.moved_vertices + 5 * res.marked_edges)
 
 
 def whole_job(dist, seconds, units, device):
@@ -812,7 +814,9 @@ def main():
                 "gpu_launches": 3 * args.steps, "batched": batched, "serving": serving, "autotune": tune,
                 "run": {"iterations": last.iterations, "traversed_edges_per_step": last.traversed_edges,
                         "processed_vertices_per_step": last.processed_vertices,
-                        "moved_vertices_per_step": last.moved_vertices, "loop_ms": last.loop_ms,
+                        "moved_vertices_per_step": last.moved_vertices, "moved_edges_per_step": last.moved_edges,
+                        "marked_edges_per_step": last.marked_edges, "dense_iterations": last.dense_iterations,
+                        "loop_ms": last.loop_ms,
                         "time_ms": last.time_ms, "modularity": res_q.modularity,
                         "host_ms_per_step": [round(x, 2) for x in host_ms],
                         "memory_gb": last.memory_gb, "plan_ms": last.plan_ms,

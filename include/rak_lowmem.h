@@ -125,7 +125,26 @@ typedef struct rak_options {
   int32_t max_blocks;         /* 0: as many thread blocks as fit on the device; k > 0: the persistent
                                  launch uses at most k blocks of 256 threads (fewer vertices in
                                  flight at once; leaves SMs to other work) [0] */
-  int64_t reserved[4];
+  int32_t dense_pct;          /* -1: never; 0: default [-1]; k in 1..100: asynchronous runs of one
+                                 graph replace the pruned frontier by every vertex after heavy
+                                 iterations: when the vertices that moved in an iteration hold at
+                                 least k% of the edges, the next iteration's moves mark no
+                                 neighbours and the iteration after it processes every vertex. The
+                                 reference marks neighbours after every move (inc/rakCuda.hxx:96-103,
+                                 called at inc/rakLowmemCuda.hxx:155,225,313,413) */
+  int32_t renumber;           /* -1 or 0: default (1 for asynchronous runs on resident graphs --
+                                 rak_graph_run -- of 2^22 vertices or more and average degree 8 or
+                                 more, which pay for the copy once; otherwise 2); 1: the run works
+                                 on a copy of the graph
+                                 renumbered in the library's work order (heaviest vertices first),
+                                 built on the device once per resident graph and layout; labels keep
+                                 their values (vertex ids) and results come back in the graph's own
+                                 numbering; RAK_MODE_ASYNC and RAK_MODE_SYNC_SPLIT with vertex-id
+                                 labels (in the split mode the results equal those on the graph as
+                                 given). 2: on the graph as given. The reference runs on a copy in
+                                 its own degree-partition order (inc/rakLowmemCuda.hxx:505-519,
+                                 563-568) */
+  int64_t reserved[3];
 } rak_options;
 
 typedef struct rak_result {
@@ -146,6 +165,11 @@ typedef struct rak_result {
   float loop_ms;               /* device time of the iterations alone (the persistent kernel) */
   float reserved_f;
   double modularity;           /* when requested, else NaN */
+  uint64_t marked_edges;       /* sum over iterations of the degrees of the moved vertices whose
+                                  neighbours were marked (moved_edges less the dense iterations'
+                                  moves, rak_options.dense_pct) */
+  int32_t dense_iterations;    /* iterations whose moves marked no neighbours (dense_pct) */
+  int32_t reserved_r;
 } rak_result;
 
 typedef struct rak_ctx rak_ctx;

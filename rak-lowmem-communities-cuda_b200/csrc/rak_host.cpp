@@ -108,9 +108,10 @@ struct DevBuf {
 // Per-run device buffers, kept by a resident graph and reused while large enough.
 struct RunBufs {
   DevBuf vcom1, aff0, aff1, arrive, claim, moved, skk, skw, stats, rs;
+  DevBuf lab;   // labels of a renumbered run, in the renumbered graph's numbering
   uint64_t bytes() const {
     return vcom1.bytes + aff0.bytes + aff1.bytes + arrive.bytes + claim.bytes + moved.bytes + skk.bytes +
-           skw.bytes + stats.bytes + rs.bytes;
+           skw.bytes + stats.bytes + rs.bytes + lab.bytes;
   }
 };
 
@@ -144,6 +145,12 @@ struct rak_graph {
   // the reference GPU path's vertex order (asynchronous runs name labels by position in it)
   rak_host_detail::DevBuf ref_ks, ref_pos;
   bool ref_ready = false;
+  // the graph renumbered in the plan's work order (rak_options.renumber), built at the first run
+  // that uses it: old -> new ids, offsets, targets, weights, and the identity work order
+  rak_host_detail::DevBuf rn_inv, rn_off, rn_tgt, rn_wt, rn_ident;
+  bool rn_ready = false;
+  rak::Layout rn_ly{0, 0, 0};
+  uint64_t rn_bytes() const { return rn_inv.bytes + rn_off.bytes + rn_tgt.bytes + rn_wt.bytes + rn_ident.bytes; }
 };
 
 struct rak_batch {
@@ -227,6 +234,9 @@ struct Resolved {
   int tie_until;         // iterations with hashed Misra-Gries ties
   int stage;             // edge staging through shared memory
   int max_blocks;        // cap on the persistent launch's blocks (0: none)
+  int dense_pct;         // rak_options.dense_pct as given (rak::dense_threshold resolves it)
+  int renumber;          // runs on the graph renumbered in work order: 0 no, 1 large graphs, 2 yes
+  bool one_shot = false; // rak_lowmem_cuda: the graph (and a renumbered copy) is built for one call
   Layout ly;
 };
 
@@ -288,6 +298,15 @@ rak_status resolve(rak_ctx *ctx, const rak_options *o, Resolved *r) {
   r->stage = stg == 1;
   if (o->max_blocks < 0) { set_err(ctx, "max_blocks must be >= 0"); return RAK_ERR_INVALID_ARGUMENT; }
   r->max_blocks = o->max_blocks;
+  if (o->dense_pct > 100) { set_err(ctx, "dense_pct must be <= 100"); return RAK_ERR_INVALID_ARGUMENT; }
+  r->dense_pct = o->dense_pct;
+  // renumbered runs: the asynchronous default; the synchronous split mode on request (its results
+  // are those of the graph as given, bit for bit, under the reference's tie rule); never the exact
+  // synchronous mode, nor runs labelled by the reference order
+  if (o->renumber > 2) { set_err(ctx, "renumber must be -1, 0, 1 or 2"); return RAK_ERR_INVALID_ARGUMENT; }
+  if (r->mode == RAK_MODE_SYNC || r->order != 1 || o->renumber == 2) r->renumber = 0;
+  else if (o->renumber == 1) r->renumber = 2;
+  else r->renumber = r->mode == RAK_MODE_ASYNC ? 1 : 0;
   r->timeout_ns = o->wait_timeout_ns > 0 ? (long long)o->wait_timeout_ns : rak::DEFAULT_WAIT_TIMEOUT_NS;
   r->start = o->start_iteration;
   r->validate = o->validate;
@@ -510,6 +529,41 @@ rak_status graph_create(rak_ctx *ctx, const rak_csr *g, const Resolved &r, Track
   return RAK_OK;
 }
 
+// The renumbered copy of a resident graph (rak_renumber.cu), for the graph's current layout.
+rak_status ensure_renumbered(rak_ctx *ctx, rak_graph *gr, Tracker *tr) {
+  if (gr->rn_ready && same_layout(gr->rn_ly, gr->ly)) return RAK_OK;
+  cudaStream_t st = ctx->stream;
+  const int64_t n = gr->n, m = gr->m;
+  const size_t ob = gr->off64 ? 8 : 4;
+  Events ev;
+  cudaEventRecord(ev.e[0], st);
+  RAK_TRY(ctx, ensure(gr->rn_inv, size_t(n) * 4));
+  RAK_TRY(ctx, ensure(gr->rn_ident, size_t(n) * 4));
+  RAK_TRY(ctx, ensure(gr->rn_off, size_t(n + 1) * ob));
+  RAK_TRY(ctx, ensure(gr->rn_tgt, size_t(m) * 4));
+  if (gr->wt) RAK_TRY(ctx, ensure(gr->rn_wt, size_t(m) * 4));
+  if (tr) tr->add(gr->rn_bytes());   // counted while the build's own space is held
+  DevBuf deg, temp;
+  RAK_TRY(ctx, deg.alloc(size_t(n + 1) * ob, tr));
+  size_t tb = 0;
+  RAK_TRY(ctx, rak::renumber_graph(gr->off, gr->off64, gr->tgt, gr->wt, gr->order, n, gr->rg.vbegin[rak::REG_LANE],
+                                   gr->rn_inv.as<uint32_t>(), deg.p, gr->rn_off.p, gr->rn_tgt.as<uint32_t>(),
+                                   gr->wt ? gr->rn_wt.as<float>() : nullptr, gr->rn_ident.as<uint32_t>(), nullptr,
+                                   &tb, st));
+  RAK_TRY(ctx, temp.alloc(tb, tr));
+  RAK_TRY(ctx, rak::renumber_graph(gr->off, gr->off64, gr->tgt, gr->wt, gr->order, n, gr->rg.vbegin[rak::REG_LANE],
+                                   gr->rn_inv.as<uint32_t>(), deg.p, gr->rn_off.p, gr->rn_tgt.as<uint32_t>(),
+                                   gr->wt ? gr->rn_wt.as<float>() : nullptr, gr->rn_ident.as<uint32_t>(), temp.p,
+                                   &tb, st));
+  cudaEventRecord(ev.e[1], st);
+  RAK_TRY(ctx, cudaStreamSynchronize(st));
+  if (tr) tr->sub(gr->rn_bytes());
+  gr->plan_ms += ev.ms(0, 1);
+  gr->rn_ready = true;
+  gr->rn_ly = gr->ly;
+  return RAK_OK;
+}
+
 // The complete run on a resident graph; labels end up in vcom0 (caller-provided, n entries).
 rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const uint8_t *flags,
                         const Resolved &r, uint32_t *vcom0, Tracker *tr, rak_result *res) {
@@ -532,6 +586,17 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
   RAK_TRY(ctx, ensure(b.skw, nc * size_t(r.slots) * 4));
   RAK_TRY(ctx, ensure(b.stats, size_t(iters) * rak::STATS_STRIDE * 8));
   RAK_TRY(ctx, ensure(b.rs, sizeof(rak::RunStateHost)));
+  // asynchronous id-label runs work on the graph renumbered in work order (rak_renumber.cu)
+  // by default only resident graphs, run again and again, pay for the copy (R-MAT scale 27: about
+  // 80 ms once, 26 ms less per run), and only large dense ones: on a sparse R-MAT (scale 25, average
+  // degree 8) the copy made runs slower (8.4 -> 10.6 ms), on the 2^25 lattice 4% faster
+  const bool renum = r.iters > 0 && n > 0 &&
+                     (r.renumber == 2 || (r.renumber == 1 && !r.one_shot && rak::mark_test_for(n, gr->m)));
+  if (renum) {
+    RAK_TRY(ctx, ensure(b.lab, size_t(n) * 4));
+    RAK_CHECK(ensure_renumbered(ctx, gr, tr));
+    if (tr) tr->add(gr->rn_bytes());
+  }
   if (tr) tr->add(b.bytes());
 
   rak::LpaArgs a{};
@@ -544,6 +609,12 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
   a.stats = b.stats.as<unsigned long long>(); a.rs = b.rs.p;
   a.iters = r.iters; a.start_iter = r.start; a.tolerance = r.tol; a.pickless_step = r.pickless;
   a.check_on_pickless = r.check_on_pickless; a.rescan = r.rescan; a.mark_test = rak::mark_test_for(a.n, gr->m); a.gpu_rule = r.rule == 2; a.timeout_ns = r.timeout_ns; a.tie_until = r.tie_until; a.stage = r.stage; a.grid_cap = r.max_blocks;
+  a.dense_moved_edges = rak::dense_threshold(r.mode, r.dense_pct, gr->m);
+  if (renum) {
+    a.off = gr->rn_off.p; a.tgt = gr->rn_tgt.as<uint32_t>(); a.wt = gr->wt ? gr->rn_wt.as<float>() : nullptr;
+    a.order = gr->rn_ident.as<uint32_t>();
+    a.vcom0 = b.lab.as<uint32_t>();
+  }
 
   // the kernel's module is loaded here, not inside the timed region
   if (r.iters > 0) RAK_TRY(ctx, rak::prepare_lpa(r.slots, r.mode, gr->off64, gr->wt == nullptr, false, r.stage));
@@ -573,10 +644,16 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
     RAK_TRY(ctx, cudaMemsetAsync(b.stats.p, 0, b.stats.bytes, st));
     RAK_TRY(ctx, cudaMemsetAsync(b.rs.p, 0, b.rs.bytes, st));
     cudaEventRecord(ev.e[0], st);
-    if (ref_labels) RAK_TRY(ctx, rak::launch_init_mapped(vcom0, q, gr->ref_pos.as<uint32_t>(), n, st));
+    if (renum) {
+      RAK_TRY(ctx, rak::launch_renumbered_init(gr->order, q, flags, n, a.vcom0, a.aff0, st));
+      if (sync) {
+        RAK_TRY(ctx, cudaMemcpyAsync(a.vcom1, a.vcom0, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
+        RAK_TRY(ctx, cudaMemsetAsync(a.aff1, 0, size_t(n), st));
+      }
+    } else if (ref_labels) RAK_TRY(ctx, rak::launch_init_mapped(vcom0, q, gr->ref_pos.as<uint32_t>(), n, st));
     else RAK_TRY(ctx, rak::launch_init(vcom0, sync ? a.vcom1 : nullptr, q, n, st));
     cudaEventRecord(ev.e[1], st);
-    RAK_TRY(ctx, rak::launch_init_flags(a.aff0, sync ? a.aff1 : nullptr, flags, n, st));
+    if (!renum) RAK_TRY(ctx, rak::launch_init_flags(a.aff0, sync ? a.aff1 : nullptr, flags, n, st));
     cudaEventRecord(ev.e[2], st);
     if (r.iters > 0) {
       int grid = 0;
@@ -597,8 +674,9 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
     return rak_status(hs.error);
   }
   const int done = r.iters > 0 ? int(hs.iterations) : 0;
-  if (sync && (done & 1)) RAK_TRY(ctx, cudaMemcpyAsync(vcom0, a.vcom1, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
+  if (sync && (done & 1)) RAK_TRY(ctx, cudaMemcpyAsync(a.vcom0, a.vcom1, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
   if (ref_labels) RAK_TRY(ctx, rak::launch_labels_to_ids(vcom0, gr->ref_ks.as<uint32_t>(), n, st));
+  if (renum) RAK_TRY(ctx, rak::launch_renumbered_gather(b.lab.as<uint32_t>(), gr->rn_inv.as<uint32_t>(), n, vcom0, st));
   RAK_TRY(ctx, cudaStreamSynchronize(st));
   if (res) {
     res->iterations = done;
@@ -606,16 +684,20 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
     res->initialization_time_ms = t_init / float(r.repeat);
     res->marking_time_ms = t_mark / float(r.repeat);
     res->loop_ms = t_loop / float(r.repeat);
-    res->traversed_edges = res->processed_vertices = res->moved_vertices = res->moved_edges = 0;
+    res->traversed_edges = res->processed_vertices = res->moved_vertices = res->moved_edges = res->marked_edges = 0;
+    res->dense_iterations = 0;
     for (int i = 0; i < done; ++i) {
       const unsigned long long *st_i = &stats[size_t(i) * rak::STATS_STRIDE];
       res->traversed_edges += st_i[rak::STAT_EDGES];
       res->processed_vertices += st_i[rak::STAT_PROCESSED];
       res->moved_vertices += st_i[rak::STAT_CHANGED];
       res->moved_edges += st_i[rak::STAT_MOVED_EDGES];
+      if (st_i[rak::STAT_PHASE] & 1ull) res->dense_iterations += 1;
+      else res->marked_edges += st_i[rak::STAT_MOVED_EDGES];
     }
     res->changed_last = done > 0 ? stats[size_t(done - 1) * rak::STATS_STRIDE + rak::STAT_CHANGED] : 0;
-    res->memory_gb = float(double(b.bytes() + size_t(n) * 4 + gr->plan_bytes) / (1024.0 * 1024.0 * 1024.0));
+    res->memory_gb = float(double(b.bytes() + size_t(n) * 4 + gr->plan_bytes + (renum ? gr->rn_bytes() : 0)) /
+                           (1024.0 * 1024.0 * 1024.0));
     res->plan_ms = gr->plan_ms;
   }
   return RAK_OK;
@@ -757,7 +839,9 @@ rak_status rak_graph_destroy(rak_graph *gr) {
   return RAK_OK;
 }
 
-uint64_t rak_graph_device_bytes(const rak_graph *gr) { return gr ? gr->graph_bytes + gr->plan_bytes : 0; }
+uint64_t rak_graph_device_bytes(const rak_graph *gr) {
+  return gr ? gr->graph_bytes + gr->plan_bytes + gr->rn_bytes() : 0;
+}
 
 rak_status rak_graph_run(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const rak_options *o,
                          uint32_t *membership, rak_result *res) {
@@ -785,6 +869,7 @@ rak_status rak_lowmem_cuda(rak_ctx *ctx, const rak_csr *g, const uint32_t *q, co
   if (!ctx || !g || !membership) return RAK_ERR_INVALID_ARGUMENT;
   Resolved r;
   RAK_CHECK(resolve(ctx, o, &r));
+  r.one_shot = true;   // the graph lives for this call only
   RAK_TRY(ctx, cudaSetDevice(ctx->device));
   rak_result tmp{};
   rak_result *rr = res ? res : &tmp;
@@ -1307,6 +1392,7 @@ rak_status rak_batch_results(rak_ctx *ctx, rak_batch *b, int32_t *iterations, ra
       total->processed_vertices += x[rak::STAT_PROCESSED];
       total->moved_vertices += x[rak::STAT_CHANGED];
       total->moved_edges += x[rak::STAT_MOVED_EDGES];
+      total->marked_edges += x[rak::STAT_MOVED_EDGES];   // batches mark after every move
     }
     total->changed_last = done > 0 ? st[size_t(done - 1) * rak::STATS_STRIDE + rak::STAT_CHANGED] : 0;
     total->plan_ms = b->g->plan_ms;

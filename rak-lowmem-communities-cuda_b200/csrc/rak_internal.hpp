@@ -61,6 +61,8 @@ constexpr int64_t MAX_LANE_MAX = 1024;
 constexpr int DEFAULT_TIE_ITERATIONS = 2;
 // Edge staging (rak_options.edge_staging) when the option is 0: 1 on, 2 off.
 constexpr int DEFAULT_EDGE_STAGING = 2;
+// Dense iterations (rak_options.dense_pct) when the option is 0; a value <= 0 means never.
+constexpr int DEFAULT_DENSE_PCT = -1;
 // Bound on each device-side wait when rak_options.wait_timeout_ns is 0.
 constexpr long long DEFAULT_WAIT_TIMEOUT_NS = 20LL * 1000 * 1000 * 1000;
 
@@ -124,9 +126,20 @@ struct LpaArgs {
   int check_on_pickless;
   int rescan;
   long long timeout_ns;
+  // asynchronous single graphs: an iteration marks no neighbours (and the next processes every
+  // vertex) when the previous iteration's moved vertices hold at least this many edges; 0: never
+  unsigned long long dense_moved_edges;
 };
 
 enum Mode { MODE_ASYNC = 0, MODE_SYNC = 1, MODE_SPLIT = 2 };
+
+// Edges that the moved vertices of an iteration must hold for the next iteration of an
+// asynchronous single-graph run to mark no neighbours (LpaArgs::dense_moved_edges); 0: never.
+inline unsigned long long dense_threshold(int mode, int pct_option, int64_t m) {
+  const int pct = pct_option == 0 ? DEFAULT_DENSE_PCT : pct_option;
+  if (mode != MODE_ASYNC || pct <= 0 || m <= 0) return 0ull;
+  return (unsigned long long)((m * int64_t(pct) + 99) / 100);
+}
 
 // Label order (rak_options.label_order) of single-graph runs when the option is 0: vertex ids (1),
 // except asynchronous runs with one or two slots, which take the reference GPU path's order (2).
@@ -138,7 +151,10 @@ enum Mode { MODE_ASYNC = 0, MODE_SYNC = 1, MODE_SPLIT = 2 };
 inline int default_label_order(int mode, int slots) { return mode == MODE_ASYNC && slots <= 2 ? 2 : 1; }
 
 // Per-iteration counters written by the LPA kernel.
-enum Stat { STAT_CHANGED = 0, STAT_EDGES = 1, STAT_PROCESSED = 2, STAT_HUBS_MOVED = 3, STAT_MOVED_EDGES = 4, STAT_WORK = 5 };
+// STAT_PHASE: how the iteration treated the frontier (bit 0: its moves marked no neighbours; bit 1:
+// it processed every vertex), written by the asynchronous single-graph kernel.
+enum Stat { STAT_CHANGED = 0, STAT_EDGES = 1, STAT_PROCESSED = 2, STAT_HUBS_MOVED = 3, STAT_MOVED_EDGES = 4, STAT_WORK = 5,
+            STAT_PHASE = 6 };
 constexpr int STATS_STRIDE = 8;
 
 // Persistent cooperative launch of all iterations; grid chosen from occupancy. `batch` selects the
@@ -183,6 +199,18 @@ size_t ref_order_scratch_bytes(int64_t n, int64_t ngraphs);
 cudaError_t ref_order(const void *off, bool off64, int64_t n, const uint32_t *gid, const int64_t *vbase,
                       int64_t ngraphs, uint32_t *ks, uint32_t *pos, void *scratch, cudaStream_t st);
 cudaError_t launch_init_mapped(uint32_t *vcom0, const uint32_t *q, const uint32_t *pos, int64_t n, cudaStream_t st);
+// rak_renumber.cu: a copy of a graph renumbered in its plan's work order (new vertex i = order[i]);
+// inv: old -> new; noff (n+1 entries), ntgt (m), nwt (m, or null for unit weights); ident: 0..n-1;
+// deg: n+1 entries of the offset type. temp null: *temp_bytes receives the scan's space.
+cudaError_t renumber_graph(const void *off, bool off64, const uint32_t *tgt, const float *wt, const uint32_t *order,
+                           int64_t n, int64_t split, uint32_t *inv, void *deg, void *noff, uint32_t *ntgt, float *nwt,
+                           uint32_t *ident, void *temp, size_t *temp_bytes, cudaStream_t st);
+// Labels (q[order[i]] or order[i]) and flags (flags[order[i]] or 1) of new vertex i.
+cudaError_t launch_renumbered_init(const uint32_t *order, const uint32_t *q, const uint8_t *flags, int64_t n,
+                                   uint32_t *lab, uint8_t *aff, cudaStream_t st);
+// out[v] = lab[inv[v]]: a run's labels back in the numbering of the graph as given.
+cudaError_t launch_renumbered_gather(const uint32_t *lab, const uint32_t *inv, int64_t n, uint32_t *out,
+                                     cudaStream_t st);
 cudaError_t launch_labels_to_ids(uint32_t *m, const uint32_t *ks, int64_t n, cudaStream_t st);
 cudaError_t launch_hub_degrees(const void *off, bool off64, const uint32_t *order, int64_t nhub,
                                int64_t *deg, cudaStream_t st);

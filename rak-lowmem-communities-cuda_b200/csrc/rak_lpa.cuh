@@ -38,6 +38,15 @@ struct Counters {
   unsigned int processed;
 };
 
+// How an asynchronous iteration treats the frontier (LpaArgs::dense_moved_edges). all: every
+// vertex is processed, whatever its flag (the previous iteration marked no neighbours); nomark:
+// moved vertices mark no neighbours (the next iteration processes every vertex). Both false in
+// the other modes and in batches: the reference's pruning, flags marked by every move.
+struct Phase {
+  bool all;
+  bool nomark;
+};
+
 template <class O>
 struct G_ {
   const O *off;
@@ -620,7 +629,7 @@ __device__ __forceinline__ void choose(const LpaArgs &a, const Sketch<S> &sk, ui
 // lane has work; region 6 is sorted by degree, so a batch holds vertices of similar degree.
 template <int S, int MODE, class O, bool UNIT, bool BATCH>
 __device__ __forceinline__ int lane_collect(const LpaArgs &a, const Regions &rg, int64_t local, const uint32_t *vin,
-                                            uint32_t *vout, const uint8_t *fin, uint32_t *q, int qn) {
+                                            uint32_t *vout, const uint8_t *fin, uint32_t *q, int qn, Phase ph) {
   const int lane = threadIdx.x & 31;
   const int64_t idx = local * 32 + lane;
   bool act = false;
@@ -628,7 +637,7 @@ __device__ __forceinline__ int lane_collect(const LpaArgs &a, const Regions &rg,
   if (idx < rg.vcount[REG_LANE]) {
     u = __ldg(a.order + rg.vbegin[REG_LANE] + idx);
     uint32_t gi, base;
-    act = fin[u] != 0 && !graph_of<BATCH>(a, u, gi, base);
+    act = (ph.all || fin[u] != 0) && !graph_of<BATCH>(a, u, gi, base);
     if constexpr (MODE != MODE_ASYNC)
       if (!act) vout[u] = vin[u];
   }
@@ -641,7 +650,7 @@ __device__ __forceinline__ int lane_collect(const LpaArgs &a, const Regions &rg,
 template <int S, int MODE, class O, bool UNIT, bool BATCH, int RULE>
 __device__ __forceinline__ void lane_batch(const LpaArgs &a, const G_<O> &g, const uint32_t *q, int count,
                                            int it, bool pickless, const uint32_t *vin, uint32_t *vout,
-                                           uint8_t *fin, uint8_t *fout, Counters &cnt) {
+                                           uint8_t *fin, uint8_t *fout, Counters &cnt, Phase ph) {
   const int lane = threadIdx.x & 31;
   if (lane >= count) return;
   const uint32_t u = q[lane];
@@ -672,6 +681,7 @@ __device__ __forceinline__ void lane_batch(const LpaArgs &a, const G_<O> &g, con
     cnt.changed += 1;
     cnt.moved_edges += (unsigned long long)(ee - eb);
     count_move<BATCH>(a, gi, it);
+    if (ph.nomark) return;
     if (!vec) mark_item<S>(a, u, eb, ee, 1, g.tgt, fout, base);
     else if (mark_tested<S>(a)) mark_lane<true>(u, eb, ee, g.tgt, fout, base);
     else mark_lane<false>(u, eb, ee, g.tgt, fout, base);
@@ -682,7 +692,7 @@ __device__ __forceinline__ void lane_batch(const LpaArgs &a, const G_<O> &g, con
 template <int S, int MODE, class O, bool UNIT, bool BATCH, int RULE>
 __device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, const G_<O> &g, int r, int64_t local,
                                            int it, bool pickless, const uint32_t *vin, uint32_t *vout,
-                                           uint8_t *fin, uint8_t *fout, Counters &cnt, StageCtx &sc) {
+                                           uint8_t *fin, uint8_t *fout, Counters &cnt, StageCtx &sc, Phase ph) {
   const int G = region_group(r);
   const int lane = threadIdx.x & 31, grp = lane / G, s = lane & (G - 1);
   const int64_t idx = local * (32 / G) + grp;
@@ -693,7 +703,7 @@ __device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, 
   if (valid) {
     u = __ldg(a.order + rg.vbegin[r] + idx);
     d = vin[u];
-    active = fin[u] != 0 && !graph_of<BATCH>(a, u, gi, base);
+    active = (ph.all || fin[u] != 0) && !graph_of<BATCH>(a, u, gi, base);
     if (active) { eb = int64_t(__ldg(g.off + u)); ee = int64_t(__ldg(g.off + u + 1)); }
   }
   Sketch<S> sk;
@@ -723,7 +733,7 @@ __device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, 
     }
     if (moved) { cnt.changed += 1; cnt.moved_edges += (unsigned long long)(ee - eb); count_move<BATCH>(a, gi, it); }
   }
-  if (moved) mark_item<S>(a, u, eb + s, ee, G, g.tgt, fout, base);
+  if (moved && !ph.nomark) mark_item<S>(a, u, eb + s, ee, G, g.tgt, fout, base);
 }
 
 // Region 0: one chunk of a split vertex per item. In the synchronous exact mode chunk 0's warp
@@ -734,7 +744,7 @@ __device__ __forceinline__ void group_item(const LpaArgs &a, const Regions &rg, 
 template <int S, int MODE, class O, bool UNIT, bool BATCH, int RULE>
 __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, const G_<O> &g, int64_t local, int it, bool pickless,
                                          const uint32_t *vin, uint32_t *vout, uint8_t *fin, uint8_t *fout,
-                                         Counters &cnt, StageCtx &sc) {
+                                         Counters &cnt, StageCtx &sc, Phase ph) {
   const int lane = threadIdx.x & 31;
   const uint32_t h = __ldg(a.chunk_hub + local);
   const int64_t first = __ldg(a.hub_first + h), nch = __ldg(a.hub_first + h + 1) - first, j = local - first;
@@ -774,7 +784,7 @@ __device__ __forceinline__ void hub_item(const LpaArgs &a, const Regions &rg, co
         const unsigned int tag = unsigned(it + 1);
         unsigned int cur = *(volatile unsigned int *)(a.hub_claim + h);
         if ((cur >> 1) != tag) {
-          const unsigned int want = (tag << 1) | (*(volatile uint8_t *)(fin + u) ? 1u : 0u);
+          const unsigned int want = (tag << 1) | (ph.all || *(volatile uint8_t *)(fin + u) ? 1u : 0u);
           const unsigned int prev = atomicCAS(a.hub_claim + h, cur, want);
           if (prev == cur) {
             cur = want;
@@ -902,8 +912,22 @@ __global__ void __launch_bounds__(256, RAK_MIN_BLOCKS) lpa_run(const LpaArgs a) 
     }
   }
   unsigned int epoch = 0;
+  // Dense iterations (asynchronous single-graph runs with LpaArgs::dense_moved_edges > 0): when
+  // the vertices that moved in the previous iteration hold at least that many edges, this
+  // iteration's moves mark no neighbours and the next iteration processes every vertex. Such a
+  // frontier would hold nearly every vertex anyway, and the marking it saves is a re-read of each
+  // moved vertex's edges plus a random flag access per edge. Decided from the previous iteration's
+  // counter, which every block reads after the barrier, so all blocks agree.
+  Phase ph{false, false};
   for (int it = 0; it < a.iters; ++it) {
     if (threadIdx.x < 4) blk[threadIdx.x] = 0;
+    if constexpr (MODE == MODE_ASYNC && !BATCH) {
+      ph.all = ph.nomark;
+      ph.nomark = a.dense_moved_edges > 0 && it > 0 &&
+                  __ldcg(a.stats + STATS_STRIDE * (it - 1) + STAT_MOVED_EDGES) >= a.dense_moved_edges;
+      if (blockIdx.x == 0 && threadIdx.x == 0)
+        a.stats[STATS_STRIDE * it + STAT_PHASE] = (ph.all ? 2ull : 0ull) | (ph.nomark ? 1ull : 0ull);
+    }
     __syncthreads();
     const int l = a.start_iter + it;
     const bool pickless = a.pickless_step > 0 && l % a.pickless_step == 0;
@@ -929,9 +953,9 @@ __global__ void __launch_bounds__(256, RAK_MIN_BLOCKS) lpa_run(const LpaArgs a) 
         for (int64_t sb = 0; sb < rg.lane_item; ++sb) {
           const int64_t sub = local * rg.lane_item + sb;
           if (sub * 32 >= rg.vcount[REG_LANE]) break;
-          qn = lane_collect<S, MODE, O, UNIT, BATCH>(a, rg, sub, vin, vout, fin, q, qn);
+          qn = lane_collect<S, MODE, O, UNIT, BATCH>(a, rg, sub, vin, vout, fin, q, qn, ph);
           if (qn >= 32) {
-            RAK_BY_RULE(lane_batch, (a, g, q, 32, it, pickless, vin, vout, fin, fout, cnt));
+            RAK_BY_RULE(lane_batch, (a, g, q, 32, it, pickless, vin, vout, fin, fout, cnt, ph));
             __syncwarp();
             if (lane < qn - 32) q[lane] = q[32 + lane];
             __syncwarp();
@@ -939,12 +963,12 @@ __global__ void __launch_bounds__(256, RAK_MIN_BLOCKS) lpa_run(const LpaArgs a) 
           }
         }
       } else if (r == REG_HUB) {
-        RAK_BY_RULE(hub_item, (a, rg, g, local, it, pickless, vin, vout, fin, fout, cnt, sc));
+        RAK_BY_RULE(hub_item, (a, rg, g, local, it, pickless, vin, vout, fin, fout, cnt, sc, ph));
       } else {
-        RAK_BY_RULE(group_item, (a, rg, g, r, local, it, pickless, vin, vout, fin, fout, cnt, sc));
+        RAK_BY_RULE(group_item, (a, rg, g, r, local, it, pickless, vin, vout, fin, fout, cnt, sc, ph));
       }
     }
-    if (qn > 0) RAK_BY_RULE(lane_batch, (a, g, q, qn, it, pickless, vin, vout, fin, fout, cnt));
+    if (qn > 0) RAK_BY_RULE(lane_batch, (a, g, q, qn, it, pickless, vin, vout, fin, fout, cnt, ph));
     __syncwarp();
     const unsigned long long ch = warp_sum((unsigned long long)cnt.changed);
     const unsigned long long ed = warp_sum(cnt.edges);
@@ -968,7 +992,8 @@ __global__ void __launch_bounds__(256, RAK_MIN_BLOCKS) lpa_run(const LpaArgs a) 
     const bool done = !BATCH && (it + 1 >= a.iters || (test && double(changed) / double(a.n) <= a.tolerance));
     // The synchronous split mode completes the next flags even on the last iteration, so a
     // single step returns them whole.
-    if (MODE != MODE_SYNC && (!done || MODE == MODE_SPLIT) && a.nchunks > 0 && __ldcg(a.stats + STATS_STRIDE * it + STAT_HUBS_MOVED) > 0) {
+    if (MODE != MODE_SYNC && !ph.nomark && (!done || MODE == MODE_SPLIT) && a.nchunks > 0 &&
+        __ldcg(a.stats + STATS_STRIDE * it + STAT_HUBS_MOVED) > 0) {
       // Second phase: neighbours of split vertices that moved this iteration.
       for (int64_t i = gw; i < a.nchunks; i += nw) {
         const uint32_t h = __ldg(a.chunk_hub + i);

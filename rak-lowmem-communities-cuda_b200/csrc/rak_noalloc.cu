@@ -137,7 +137,7 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   if (order_kind == 2 && sync) return RAK_ERR_UNSUPPORTED;
   const int iters = o->max_iterations;
   if (iters < 0 || iters > 1024 || !(o->tolerance >= 0) || o->wait_timeout_ns < 0) return RAK_ERR_INVALID_ARGUMENT;
-  if (o->tie_break > 2 || o->tie_iterations < 0 || o->edge_staging > 2) return RAK_ERR_INVALID_ARGUMENT;
+  if (o->tie_break > 2 || o->tie_iterations < 0 || o->edge_staging > 2 || o->dense_pct > 100) return RAK_ERR_INVALID_ARGUMENT;
   if (o->tie_break == 2 && o->sketch_rule == 2) return RAK_ERR_UNSUPPORTED;
   Layout ly;
   ly.lane_max = o->lane_max > 0 ? o->lane_max : DEFAULT_LANE_MAX;
@@ -295,6 +295,7 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
   a.stage = stage;
   a.grid_cap = o->max_blocks > 0 ? o->max_blocks : 0;
   a.timeout_ns = o->wait_timeout_ns > 0 ? (long long)o->wait_timeout_ns : DEFAULT_WAIT_TIMEOUT_NS;
+  a.dense_moved_edges = dense_threshold(mode, o->dense_pct, g->m);
   if (iters > 0) {
     int grid = 0;
     NA_TRY(launch_lpa(a, slots, mode, off64, st, &grid));
@@ -325,6 +326,8 @@ extern "C" rak_status rak_lowmem_cuda_noalloc(int device, void *stream, const ra
     rr->processed_vertices += x[STAT_PROCESSED];
     rr->moved_vertices += x[STAT_CHANGED];
     rr->moved_edges += x[STAT_MOVED_EDGES];
+    if (x[STAT_PHASE] & 1ull) rr->dense_iterations += 1;
+    else rr->marked_edges += x[STAT_MOVED_EDGES];
   }
   rr->changed_last = done > 0 ? sh[size_t(done - 1) * STATS_STRIDE + STAT_CHANGED] : 0;
   rr->peak_device_bytes = cv.need;

@@ -45,7 +45,8 @@ class rak_options(C.Structure):
                 ("compute_modularity", C.c_int32), ("start_iteration", C.c_int32),
                 ("initial_flags", C.c_void_p), ("sketch_rule", C.c_int32), ("label_order", C.c_int32),
                 ("wait_timeout_ns", C.c_int64), ("tie_break", C.c_int32), ("tie_iterations", C.c_int32),
-                ("edge_staging", C.c_int32), ("max_blocks", C.c_int32), ("reserved", C.c_int64 * 4)]
+                ("edge_staging", C.c_int32), ("max_blocks", C.c_int32), ("dense_pct", C.c_int32),
+                ("renumber", C.c_int32), ("reserved", C.c_int64 * 3)]
 
 
 class rak_result(C.Structure):
@@ -54,7 +55,8 @@ class rak_result(C.Structure):
                 ("h2d_ms", C.c_float), ("d2h_ms", C.c_float), ("peak_device_bytes", C.c_uint64),
                 ("traversed_edges", C.c_uint64), ("processed_vertices", C.c_uint64),
                 ("changed_last", C.c_uint64), ("moved_vertices", C.c_uint64), ("moved_edges", C.c_uint64),
-                ("loop_ms", C.c_float), ("reserved_f", C.c_float), ("modularity", C.c_double)]
+                ("loop_ms", C.c_float), ("reserved_f", C.c_float), ("modularity", C.c_double),
+                ("marked_edges", C.c_uint64), ("dense_iterations", C.c_int32), ("reserved_r", C.c_int32)]
 
 
 class rak_batch_csr(C.Structure):
@@ -229,6 +231,9 @@ class Result:
     loop_ms: float
     reserved_f: float
     modularity: float
+    marked_edges: int
+    dense_iterations: int
+    reserved_r: int
 
     @staticmethod
     def of(r: rak_result) -> "Result":
