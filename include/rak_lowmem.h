@@ -372,7 +372,8 @@ rak_status rak_server_destroy(rak_server *s);
  * Graphs whose buffers exceed the array (roughly 20 bytes per vertex, 28 with the reference label
  * order that asynchronous runs use by default, plus 8*slots bytes per split chunk) return
  * RAK_ERR_OUT_OF_MEMORY with res->peak_device_bytes set to the bytes needed. Options and labels
- * mean what they mean for rak_lowmem_cuda.
+ * mean what they mean for rak_lowmem_cuda, except rak_options.renumber: runs here always work on
+ * the graph as given (a renumbered copy would not fit the array).
  * The first call on a device looks the array up on that device (make it before any stream
  * capture). CUDA places the array, and each kernel variant's code (slot count, mode, offset width,
  * weighted or unit), on a device lazily, when a call first needs it; those are the runtime's own
