@@ -590,8 +590,17 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
   // by default only resident graphs, run again and again, pay for the copy (R-MAT scale 27: about
   // 80 ms once, 26 ms less per run), and only large dense ones: on a sparse R-MAT (scale 25, average
   // degree 8) the copy made runs slower (8.4 -> 10.6 ms), on the 2^25 lattice 4% faster
-  const bool renum = r.iters > 0 && n > 0 &&
-                     (r.renumber == 2 || (r.renumber == 1 && !r.one_shot && rak::mark_test_for(n, gr->m)));
+  bool renum = r.iters > 0 && n > 0 &&
+               (r.renumber == 2 || (r.renumber == 1 && !r.one_shot && rak::mark_test_for(n, gr->m)));
+  if (renum && r.renumber == 1 && !(gr->rn_ready && same_layout(gr->rn_ly, gr->ly))) {
+    // by default the copy is only made when it fits beside what the device holds, with 1 GiB to
+    // spare; otherwise the run works on the graph as given
+    size_t free_b = 0, total_b = 0;
+    const size_t need = size_t(n) * (gr->off64 ? 8 : 4) * 2 + size_t(n) * 12 + size_t(gr->m) * (gr->wt ? 8 : 4) +
+                        (size_t(1) << 30);
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { cudaGetLastError(); free_b = 0; }
+    if (free_b < need) renum = false;
+  }
   if (renum) {
     RAK_TRY(ctx, ensure(b.lab, size_t(n) * 4));
     RAK_CHECK(ensure_renumbered(ctx, gr, tr));
