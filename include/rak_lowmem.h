@@ -139,8 +139,8 @@ typedef struct rak_options {
                                  renumbered in the library's work order (heaviest vertices first),
                                  built on the device once per resident graph and layout; labels keep
                                  their values (vertex ids) and results come back in the graph's own
-                                 numbering; RAK_MODE_ASYNC and RAK_MODE_SYNC_SPLIT with vertex-id
-                                 labels (in the split mode the results equal those on the graph as
+                                 numbering; RAK_MODE_ASYNC (either label order) and
+                                 RAK_MODE_SYNC_SPLIT (whose results equal those on the graph as
                                  given). 2: on the graph as given. The reference runs on a copy in
                                  its own degree-partition order (inc/rakLowmemCuda.hxx:505-519,
                                  563-568) */

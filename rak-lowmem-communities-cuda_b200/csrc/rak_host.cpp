@@ -302,9 +302,9 @@ rak_status resolve(rak_ctx *ctx, const rak_options *o, Resolved *r) {
   r->dense_pct = o->dense_pct;
   // renumbered runs: the asynchronous default; the synchronous split mode on request (its results
   // are those of the graph as given, bit for bit, under the reference's tie rule); never the exact
-  // synchronous mode, nor runs labelled by the reference order
+  // synchronous mode
   if (o->renumber > 2) { set_err(ctx, "renumber must be -1, 0, 1 or 2"); return RAK_ERR_INVALID_ARGUMENT; }
-  if (r->mode == RAK_MODE_SYNC || r->order != 1 || o->renumber == 2) r->renumber = 0;
+  if (r->mode == RAK_MODE_SYNC || o->renumber == 2) r->renumber = 0;
   else if (o->renumber == 1) r->renumber = 2;
   else r->renumber = r->mode == RAK_MODE_ASYNC ? 1 : 0;
   r->timeout_ns = o->wait_timeout_ns > 0 ? (long long)o->wait_timeout_ns : rak::DEFAULT_WAIT_TIMEOUT_NS;
@@ -654,7 +654,8 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
     RAK_TRY(ctx, cudaMemsetAsync(b.rs.p, 0, b.rs.bytes, st));
     cudaEventRecord(ev.e[0], st);
     if (renum) {
-      RAK_TRY(ctx, rak::launch_renumbered_init(gr->order, q, flags, n, a.vcom0, a.aff0, st));
+      RAK_TRY(ctx, rak::launch_renumbered_init(gr->order, q, ref_labels ? gr->ref_pos.as<uint32_t>() : nullptr, flags,
+                                               n, a.vcom0, a.aff0, st));
       if (sync) {
         RAK_TRY(ctx, cudaMemcpyAsync(a.vcom1, a.vcom0, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
         RAK_TRY(ctx, cudaMemsetAsync(a.aff1, 0, size_t(n), st));
@@ -684,8 +685,8 @@ rak_status run_resident(rak_ctx *ctx, rak_graph *gr, const uint32_t *q, const ui
   }
   const int done = r.iters > 0 ? int(hs.iterations) : 0;
   if (sync && (done & 1)) RAK_TRY(ctx, cudaMemcpyAsync(a.vcom0, a.vcom1, size_t(n) * 4, cudaMemcpyDeviceToDevice, st));
-  if (ref_labels) RAK_TRY(ctx, rak::launch_labels_to_ids(vcom0, gr->ref_ks.as<uint32_t>(), n, st));
   if (renum) RAK_TRY(ctx, rak::launch_renumbered_gather(b.lab.as<uint32_t>(), gr->rn_inv.as<uint32_t>(), n, vcom0, st));
+  if (ref_labels) RAK_TRY(ctx, rak::launch_labels_to_ids(vcom0, gr->ref_ks.as<uint32_t>(), n, st));
   RAK_TRY(ctx, cudaStreamSynchronize(st));
   if (res) {
     res->iterations = done;

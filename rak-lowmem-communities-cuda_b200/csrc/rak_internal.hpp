@@ -205,9 +205,10 @@ cudaError_t launch_init_mapped(uint32_t *vcom0, const uint32_t *q, const uint32_
 cudaError_t renumber_graph(const void *off, bool off64, const uint32_t *tgt, const float *wt, const uint32_t *order,
                            int64_t n, int64_t split, uint32_t *inv, void *deg, void *noff, uint32_t *ntgt, float *nwt,
                            uint32_t *ident, void *temp, size_t *temp_bytes, cudaStream_t st);
-// Labels (q[order[i]] or order[i]) and flags (flags[order[i]] or 1) of new vertex i.
-cudaError_t launch_renumbered_init(const uint32_t *order, const uint32_t *q, const uint8_t *flags, int64_t n,
-                                   uint32_t *lab, uint8_t *aff, cudaStream_t st);
+// Labels (q[order[i]] or order[i], through pos when given: labels as positions in the reference
+// order) and flags (flags[order[i]] or 1) of new vertex i.
+cudaError_t launch_renumbered_init(const uint32_t *order, const uint32_t *q, const uint32_t *pos, const uint8_t *flags,
+                                   int64_t n, uint32_t *lab, uint8_t *aff, cudaStream_t st);
 // out[v] = lab[inv[v]]: a run's labels back in the numbering of the graph as given.
 cudaError_t launch_renumbered_gather(const uint32_t *lab, const uint32_t *inv, int64_t n, uint32_t *out,
                                      cudaStream_t st);

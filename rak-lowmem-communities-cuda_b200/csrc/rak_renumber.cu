@@ -81,13 +81,15 @@ __global__ void k_rn_iota(uint32_t *__restrict__ p, int64_t n) {
 }
 
 // Labels and flags of a run in the new numbering: new vertex i is order[i] of the graph as given.
+// pos (runs labelled by the reference order): a label is the position of that vertex id in it.
 __global__ void k_rn_init(const uint32_t *__restrict__ order, const uint32_t *__restrict__ q,
-                          const uint8_t *__restrict__ flags, int64_t n, uint32_t *__restrict__ lab,
-                          uint8_t *__restrict__ aff) {
+                          const uint32_t *__restrict__ pos, const uint8_t *__restrict__ flags, int64_t n,
+                          uint32_t *__restrict__ lab, uint8_t *__restrict__ aff) {
   const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, nt = int64_t(gridDim.x) * blockDim.x;
   for (int64_t i = tid; i < n; i += nt) {
     const uint32_t u = __ldg(order + i);
-    lab[i] = q ? __ldg(q + u) : u;
+    const uint32_t c = q ? __ldg(q + u) : u;
+    lab[i] = pos ? __ldg(pos + c) : c;
     aff[i] = flags ? uint8_t(__ldg(flags + u) != 0) : uint8_t(1);
   }
 }
@@ -129,9 +131,9 @@ cudaError_t renumber_graph(const void *off, bool off64, const uint32_t *tgt, con
                              temp_bytes, st);
 }
 
-cudaError_t launch_renumbered_init(const uint32_t *order, const uint32_t *q, const uint8_t *flags, int64_t n,
-                                   uint32_t *lab, uint8_t *aff, cudaStream_t st) {
-  k_rn_init<<<grid_of(n, 4), TPB, 0, st>>>(order, q, flags, n, lab, aff);
+cudaError_t launch_renumbered_init(const uint32_t *order, const uint32_t *q, const uint32_t *pos, const uint8_t *flags,
+                                   int64_t n, uint32_t *lab, uint8_t *aff, cudaStream_t st) {
+  k_rn_init<<<grid_of(n, 4), TPB, 0, st>>>(order, q, pos, flags, n, lab, aff);
   return cudaGetLastError();
 }
 

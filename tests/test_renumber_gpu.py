@@ -78,7 +78,7 @@ def test_resident_graph_keeps_one_copy_across_layouts(ctx):
     rg.close()
 
 
-@pytest.mark.parametrize("slots", [8, 1])
+@pytest.mark.parametrize("slots", [8, 1])   # 1: labels are positions in the reference order by default
 def test_async_renumbered_quality(ctx, slots):
     g = rl.gen_rmat(18, 16, seed=42)
     og = orc.Graph.of(g)
@@ -90,7 +90,7 @@ def test_async_renumbered_quality(ctx, slots):
     assert r1.modularity >= r0.modularity * 0.97 - 1e-4, (r1.modularity, r0.modularity)
 
 
-def test_exact_mode_and_reference_labels_are_not_renumbered(ctx):
+def test_exact_mode_is_not_renumbered(ctx):
     g = rl.gen_rmat(12, 8, seed=12)
     lab0, r0 = ctx.lowmem(g, mode=rl.MODE_SYNC, renumber=2)
     lab1, r1 = ctx.lowmem(g, mode=rl.MODE_SYNC, renumber=1)
