@@ -814,7 +814,11 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
-                "method": method, "step": "one whole run to convergence on the resident graph",
+                "method": method,
+                "step": "one whole run to convergence on the resident graph (labels and flags initialised, "
+                        "every iteration, labels gathered back); the graph's plan and, for large dense graphs, "
+                        "its copy renumbered in work order are built once per resident graph before the timed "
+                        "region (run.plan_ms); the e2e leg's one-shot calls build what they use inside the call",
                 "roofline": roofline, "cpu_baseline": cpu, "cpu_baseline_gve_lpa": cpu_gve, "e2e": e2e,
                 "clocks": clk.summary(),
                 "gpu_launches": 3 * args.steps, "batched": batched, "serving": serving, "autotune": tune,
