@@ -31,7 +31,7 @@ __host__ __device__ inline int64_t region_items(int r, int64_t cnt, int64_t nchu
 // 4 batches keep that counter from serialising the iteration (2D lattice 2^25: 1.06 -> 0.89 ms
 // per iteration), while a graph with few one-lane vertices needs single batches to give every
 // resident warp work (R-MAT scale 16: 2.5x slower with 4). warps: resident warps of a launch.
-constexpr int LPA_WARPS_PER_SM = 24;  // lpa_run: 256-thread blocks, 3 resident per SM
+constexpr int LPA_WARPS_PER_SM = 32;  // lpa_run: 256-thread blocks, 4 resident per SM (RAK_MIN_BLOCKS)
 inline int64_t lane_item_for(int64_t lane_vertices, int64_t warps) {
   const int64_t batches = (lane_vertices + 31) / 32, w = warps > 0 ? warps : 1;
   return batches >= 32 * w ? 4 : batches >= 16 * w ? 2 : 1;

@@ -21,12 +21,16 @@
 #include "rak_internal.hpp"
 
 // Edges loaded ahead per lane in the scan pipeline, and the resident blocks per SM the register
-// budget is sized for.
+// budget is sized for. Four blocks (64 registers; the asynchronous instantiations spill a few
+// hundred bytes) against three (80 registers), measured on B200 on renumbered resident graphs, one
+// box, runs alternated: R-MAT s27 100.5-100.7 vs 102.3-102.4 ms at lower clocks, s24 ef32 weighted
+// 30.2 vs 31.4 ms, 2D lattice 2^25 9.0 vs 9.8 ms (on the graphs as given, earlier, four blocks were
+// 1-5% slower): the loads in flight of the extra warps pay for the spills.
 #ifndef RAK_SCAN_BATCH
 #define RAK_SCAN_BATCH 4
 #endif
 #ifndef RAK_MIN_BLOCKS
-#define RAK_MIN_BLOCKS 3
+#define RAK_MIN_BLOCKS 4
 #endif
 
 namespace rak {
