@@ -98,3 +98,26 @@ def test_exact_mode_is_not_renumbered(ctx):
     with pytest.raises(rl.RakError) as e:
         ctx.lowmem(g, renumber=3)
     assert e.value.status == 1
+
+
+def test_default_copy_only_when_it_fits(ctx):
+    """The default makes the renumbered copy of a large dense resident graph only when it fits beside
+    what the device already holds (with 1 GiB to spare); otherwise the run works on the graph as
+    given. Device memory is filled with one tensor to leave too little room, then released."""
+    import torch
+    g = rl.gen_rmat(22, 16, seed=13)            # 2^22 vertices, average degree above 8: copied by default
+    rg = rl.ResidentGraph(ctx, g)
+    out = torch.empty(g.n, dtype=torch.int32, device="cuda")
+    copy_gb = (g.m * 4 + (g.n + 1) * 8 + g.n * 8) / 2**30   # targets, offsets, inverse map, work order
+    free, _ = torch.cuda.mem_get_info(0)
+    filler = torch.empty(max(0, free - (1 << 30) - (256 << 20)), dtype=torch.uint8, device="cuda")
+    r0 = rg.run(out)                            # about 1.25 GiB free: below the copy plus its margin
+    del filler
+    torch.cuda.empty_cache()
+    assert r0.memory_gb < copy_gb, (r0.memory_gb, copy_gb)
+    lab0 = out.cpu().numpy().view(np.uint32)
+    assert lab0.max() < g.n
+    r1 = rg.run(out)                            # room again: the copy is made and used
+    assert r1.memory_gb - r0.memory_gb >= 0.9 * copy_gb, (r1.memory_gb, r0.memory_gb, copy_gb)
+    assert out.cpu().numpy().view(np.uint32).max() < g.n
+    rg.close()
